@@ -1,0 +1,230 @@
+/*
+ * rtscan_b200.h -- C-ABI of the B200 multi-column range-predicate scan.
+ *
+ * This is the drop-in boundary for RTScan's scan path (AntaresAlice/RTScan).
+ * The reference has no library ABI: its path sits behind driver main()s, the
+ * column-file and scan_cmd formats, and a set of C-linkage-style CUDA host
+ * functions (bindex.h:366-376, rt.h:337-345).  Each entry point below names
+ * the reference interface it replaces.
+ *
+ * Conventions (all verified against the reference):
+ *   - Columns are uint32 values; a column file holds `ncols` columns of
+ *     `nrows` little-endian uint32 values back to back, no header
+ *     (getDataFromFile, bindex_cuda.cpp:1269-1286).
+ *   - A result bitmap is rts_bitmap_words(nrows) 32-bit words.  Row i is bit
+ *     31-(i%32) of word i>>5 ("MSB-first", bindex.cpp:269,1217;
+ *     cuda_and.cu:94-96).  Bits past row nrows-1 are always zero.
+ *   - A query is a conjunction of terms lo <= column <= hi (inclusive).  The
+ *     reference operators lt/le/gt/ge/eq/bt (raw_scan, bindex.cpp:1851-1892)
+ *     are lowered to that form by rts_lower_op; a term with lo > hi matches
+ *     nothing.
+ *   - Every call returns an rts_status: 0 on success, a negative code on
+ *     failure with a message from rts_last_error().  Nothing here calls
+ *     exit() (the reference does, e.g. cuda_and.cu:528-546).
+ *   - `stream` arguments are cudaStream_t values passed as void* (NULL = the
+ *     legacy default stream).  *_async calls only enqueue work.
+ *
+ * Threading: one rts_ctx per host thread, except the rts_server_* calls,
+ * which are safe from many producer threads.
+ */
+#ifndef RTSCAN_B200_H_
+#define RTSCAN_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTS_API __attribute__((visibility("default")))
+
+/* ---- status codes ------------------------------------------------------ */
+typedef int32_t rts_status;
+#define RTS_OK 0
+#define RTS_ERR_ARG (-1)      /* bad argument (null pointer, size, column index) */
+#define RTS_ERR_CUDA (-2)     /* a CUDA call failed; message names it */
+#define RTS_ERR_NOMEM (-3)    /* device or host allocation failed */
+#define RTS_ERR_IO (-4)       /* file missing, short or unreadable */
+#define RTS_ERR_PARSE (-5)    /* malformed scan_cmd text */
+#define RTS_ERR_STATE (-6)    /* call not valid in this state (no columns, no index) */
+#define RTS_ERR_TIMEOUT (-7)  /* a bounded wait ran out */
+#define RTS_ERR_FULL (-8)     /* admission refused: queue or result memory full */
+#define RTS_ERR_NODEV (-9)    /* no CUDA device, or not an sm_100 device */
+#define RTS_ERR_CANCELLED (-10) /* the request was cancelled */
+
+/* ---- operators: same order as the reference's OPERATOR enum (bindex.h:200-207) */
+#define RTS_OP_EQ 0
+#define RTS_OP_LT 1
+#define RTS_OP_GT 2
+#define RTS_OP_LE 3
+#define RTS_OP_GE 4
+#define RTS_OP_BT 5 /* t1 < x < t2, exclusive, bounds swapped when t1 > t2 */
+
+/* One conjunct of a query: lo <= column <= hi (inclusive). */
+typedef struct rts_term {
+  int32_t column;
+  uint32_t lo;
+  uint32_t hi;
+} rts_term;
+
+typedef struct rts_ctx rts_ctx;
+typedef struct rts_qset rts_qset;
+typedef struct rts_server rts_server;
+
+/* ---- errors and library info ------------------------------------------- */
+
+/* Message of the last failed call on `ctx`, or of the calling thread's last
+ * failed context-free call when ctx is NULL.  Never NULL. */
+RTS_API const char *rts_last_error(const rts_ctx *ctx);
+/* Library version string, e.g. "rtscan_b200 0.1 sm_100a". */
+RTS_API const char *rts_version(void);
+/* Words of a result bitmap for `nrows` rows: ceil(nrows/32)
+ * (bits_num_needed, bindex.h:334-337). */
+RTS_API uint64_t rts_bitmap_words(uint64_t nrows);
+
+/* ---- operator lowering and scan_cmd parsing ----------------------------- */
+
+/* Lower one reference operator to an inclusive range (replaces the operator
+ * dispatch of raw_scan, bindex.cpp:1851-1892, without the reference's
+ * overflow at the domain edges, bindex.cpp:1419-1427,1478-1487).
+ * *nonempty is 0 when no value can match (lt 0, gt 4294967295, bt a b with
+ * b <= a+1 after swapping). */
+RTS_API rts_status rts_lower_op(int32_t op, uint32_t t1, uint32_t t2, uint32_t *lo, uint32_t *hi,
+                                int32_t *nonempty);
+
+/* Parse scan_cmd text (replaces the query loops of bindex.cpp:2165-2189,
+ * bindex_cuda.cpp:1834-1854 and rtscan.cpp:992-1035 with stringSplit and
+ * get_target_numbers, bindex.cpp:238-245,1840-1849).  `ncols` consecutive
+ * lines form one conjunctive query, line c applying to column c; a line
+ * `exit` (or the end of the text) ends the list and text after it is
+ * ignored.  Each line is `<op> <t1>[,<t1>...] [<t2>[,<t2>...]]`, numbers
+ * parsed as doubles and converted like the reference's (CODE)stod(..).  A
+ * comma list of targets expands the query into one query per target
+ * position.  Returns RTS_ERR_PARSE with the line number on malformed text. */
+RTS_API rts_status rts_parse_scan_cmd(const char *text, uint64_t len, int32_t ncols, rts_qset **out);
+RTS_API int32_t rts_qset_size(const rts_qset *qs);
+/* Terms of query i (pointer valid until rts_qset_free).  *empty is 1 when
+ * some term can never match (then the result is all zeros). */
+RTS_API rts_status rts_qset_query(const rts_qset *qs, int32_t i, const rts_term **terms, int32_t *nterms,
+                                  int32_t *empty);
+/* The parsed operator of query i, column c, as written in the text. */
+RTS_API rts_status rts_qset_line(const rts_qset *qs, int32_t i, int32_t c, int32_t *op, uint32_t *t1,
+                                 uint32_t *t2);
+RTS_API void rts_qset_free(rts_qset *qs);
+
+/* ---- context and resident columns --------------------------------------- */
+
+/* Open a context on CUDA device `device` (replaces the hard-coded
+ * cudaSetDevice(0) of every cuda_and.cu entry point, e.g. cuda_and.cu:265). */
+RTS_API rts_status rts_open(int32_t device, rts_ctx **out);
+RTS_API void rts_close(rts_ctx *ctx);
+/* Copy `ncols` host columns of `nrows` values into HBM, where they stay
+ * resident (the rawDataInGPU upload of init_bindex_in_GPU,
+ * bindex_cuda.cpp:192-194).  Replaces any earlier table and index. */
+RTS_API rts_status rts_load_columns(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
+                                    uint64_t nrows);
+/* Read a column file (format above) into HBM (getDataFromFile,
+ * bindex_cuda.cpp:1269-1286; get_data_from_file, rtscan.cpp:336-356).
+ * nrows == 0 takes file size / (4*ncols). */
+RTS_API rts_status rts_load_file(rts_ctx *ctx, const char *path, int32_t ncols, uint64_t nrows);
+/* Borrow columns that already live on the context's device (no copy; the
+ * caller keeps them alive until the next load or rts_close). */
+RTS_API rts_status rts_attach_columns(rts_ctx *ctx, const uint32_t *const *dev_cols, int32_t ncols,
+                                      uint64_t nrows);
+RTS_API uint64_t rts_nrows(const rts_ctx *ctx);
+RTS_API int32_t rts_ncols(const rts_ctx *ctx);
+RTS_API int32_t rts_device(const rts_ctx *ctx);
+RTS_API int32_t rts_sm_count(const rts_ctx *ctx);
+RTS_API const uint32_t *rts_column_ptr(const rts_ctx *ctx, int32_t column);
+/* Number of kernels this context has launched so far. */
+RTS_API uint64_t rts_kernel_launches(const rts_ctx *ctx);
+
+/* ---- single-query scans -------------------------------------------------- */
+
+/* Fused conjunctive scan: one pass that reads every referenced column once,
+ * compares lo <= x <= hi in registers, ANDs the terms and writes the packed
+ * bitmap plus its popcount.  Replaces the per-column sieve copies, the
+ * C-1 GPUbitAndWithCuda passes (merge_with_GPU, bindex_cuda.cpp:1662-1706;
+ * cuda_and.cu:255-296) and the CPU hit count (compare_bitmap,
+ * bindex.cpp:1959-1978).  dev_bitmap: rts_bitmap_words(nrows) words on the
+ * device; *dev_count: one uint64 on the device, overwritten. */
+RTS_API rts_status rts_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
+                                  uint64_t *dev_count, void *stream);
+/* Same result by separate passes: one predicate pass per column into its own
+ * bitmap, then C-1 AND passes, then a popcount pass -- the structure of the
+ * reference's GPU path (bitmap_copy* + bit_andKernel, cuda_and.cu:13-61),
+ * kept as the comparison the multi-column benchmark asks for.  Uses
+ * context-owned scratch bitmaps. */
+RTS_API rts_status rts_scan_separate_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms,
+                                           uint32_t *dev_bitmap, uint64_t *dev_count, void *stream);
+/* Blocking scan into host memory: the best device plan for the query, then
+ * the bitmap copied to `host_bitmap` (rts_bitmap_words(nrows) words; pinned
+ * memory is fastest) and the count to *count.  host_bitmap may be NULL to
+ * fetch the count only.  (The result D2H of bindex_cuda.cpp:1932-1946.) */
+RTS_API rts_status rts_scan(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *host_bitmap,
+                            uint64_t *count);
+
+/* ---- bitmap utilities ---------------------------------------------------- */
+#define RTS_BM_AND 0    /* dst = a & b   (bit_andKernel, cuda_and.cu:13-20) */
+#define RTS_BM_OR 1     /* dst = a | b   (bit_orKernel, cuda_and.cu:23-30) */
+#define RTS_BM_COPY 2   /* dst = a       (bitmap_copyKernel, cuda_and.cu:34-41) */
+#define RTS_BM_NOT 3    /* dst = ~a      (bitmap_copyNegationKernel, cuda_and.cu:45-52) */
+#define RTS_BM_ANDNOT 4 /* dst = b & ~a  (bitmap_copySIMDKernel, cuda_and.cu:54-61) */
+#define RTS_BM_FILL 5   /* dst = value   (bitmap_memsetKernel, cuda_and.cu:65-72) */
+/* Element-wise bitmap op over `words` device words (replaces
+ * GPUbit{And,Or,Copy,CopyNegation,CopySIMD,Memset}WithCuda, bindex.h:367-372).
+ * dst may alias a.  `value` is used by RTS_BM_FILL only. */
+RTS_API rts_status rts_bitmap_op_async(rts_ctx *ctx, int32_t op, uint32_t *dst, const uint32_t *a,
+                                       const uint32_t *b, uint64_t words, uint32_t value, void *stream);
+/* Popcount of the first `nbits` bits of a device bitmap into *dev_count. */
+RTS_API rts_status rts_bitmap_count_async(rts_ctx *ctx, const uint32_t *bitmap, uint64_t nbits,
+                                          uint64_t *dev_count, void *stream);
+
+/* ---- BinDex: sieve + refine ---------------------------------------------- */
+
+/* Build the BinDex index of one column on the GPU (replaces init_bindex,
+ * bindex.cpp:599-671, and init_bindex_in_GPU, bindex_cuda.cpp:164-282):
+ * sorted values and positions, K equal-count areas with the reference's
+ * duplicate rule, and K-1 filter vectors fv[k] = (x < start value of area
+ * k+1).  K in [2, 4096]; the reference's default is 128 (VAREA_N). */
+RTS_API rts_status rts_build_bindex(rts_ctx *ctx, int32_t column, int32_t K);
+RTS_API rts_status rts_drop_bindex(rts_ctx *ctx, int32_t column);
+/* Area start values and their sorted positions (lower bounds) of a built
+ * index, for inspection: starts[K], first_rank[K] on the host. */
+RTS_API rts_status rts_bindex_areas(const rts_ctx *ctx, int32_t column, uint32_t *starts,
+                                    uint64_t *first_rank, int32_t K);
+/* Copy filter vector k (0 <= k < K-1) of a built index, rts_bitmap_words(nrows)
+ * words, into host memory (the filterVectors[k] of bindex.h:311). */
+RTS_API rts_status rts_bindex_filter_vector(rts_ctx *ctx, int32_t column, int32_t k, uint32_t *host_out);
+/* Conjunctive query through the indexes: a sieve that ANDs 1-2 filter
+ * vectors per term, then one refine launch that re-tests every row whose
+ * sieve bit may be wrong (rows between a bound and its filter-vector
+ * boundary, read from the sorted positions) on all terms, and fixes the bit
+ * and the count.  Replaces bindex_scan_{lt,gt,bt}_in_GPU (bindex_cuda.cpp:
+ * 903-1115), special_eq_scan (1450-1504), refine_with_Cuda (1506-1660) and
+ * GPURefine{,Eq}AreaWithCuda (cuda_and.cu:510-812).  Every term's column
+ * must have an index. */
+RTS_API rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms,
+                                         uint32_t *dev_bitmap, uint64_t *dev_count, void *stream);
+
+/* ---- batched scans -------------------------------------------------------- */
+
+/* Many queries in one pass (no reference counterpart; the reference runs one
+ * query per loop iteration, bindex_cuda.cpp:1827-1986).  Queries are CSR:
+ * query q owns terms[offsets[q] .. offsets[q+1]).  Query q's bitmap is
+ * dev_bitmaps + q*stride_words (stride_words >= rts_bitmap_words(nrows));
+ * its count is dev_counts[q].  The persistent kernel streams each column
+ * chunk from HBM once and evaluates every query on it. */
+RTS_API rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
+                                        int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
+                                        uint64_t *dev_counts, void *stream);
+/* The same queries with one fused-scan launch per query (the baseline the
+ * batched kernel is measured against). */
+RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
+                                       int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
+                                       uint64_t *dev_counts, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTSCAN_B200_H_ */

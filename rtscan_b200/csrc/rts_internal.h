@@ -1,0 +1,120 @@
+// Internal declarations shared by the host code and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rtscan_b200.h"
+
+namespace rts {
+
+// Rows covered by one warp-tile of the fused scan: 32 lanes x 8 vectors x
+// 4 values; its result is 32 bitmap words (one 128-byte store per warp).
+constexpr int kTileRows = 1024;
+constexpr int kTileWords = kTileRows / 32;
+// Terms one fused launch evaluates; longer queries take extra AND passes.
+constexpr int kFusedMaxTerms = 16;
+
+struct Error : std::runtime_error {
+  rts_status code;
+  Error(rts_status c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define RTS_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::rts::Error(RTS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Record `msg` as the calling thread's last error (rts_last_error(NULL)).
+rts_status set_thread_error(rts_status code, const std::string &msg);
+
+inline uint64_t words_for(uint64_t nrows) { return (nrows + 31) >> 5; }
+
+// One term of a fused launch: hit iff (x - lo) <= span, unsigned, which is
+// lo <= x <= hi for span = hi - lo.
+struct DevTerm {
+  const uint32_t *col;
+  uint32_t lo;
+  uint32_t span;
+};
+
+struct ScanParams {
+  DevTerm t[kFusedMaxTerms];
+  int nterms;
+  int and_into;  // 1: AND the result into the words already in `out`
+  uint32_t *out;
+  unsigned long long *count;  // may be null
+  uint64_t nrows;
+  uint64_t full_tiles;        // tiles of kTileRows rows entirely below nrows
+};
+
+// ---- kernel launchers (scan_kernels.cu) ----
+struct LaunchShape {
+  int blocks;
+  int threads;
+};
+void launch_scan_fused(const ScanParams &p, bool vector_ok, int sm_count, cudaStream_t s);
+void launch_bitmap_op(int op, uint32_t *dst, const uint32_t *a, const uint32_t *b, uint64_t words,
+                      uint32_t value, int sm_count, cudaStream_t s);
+void launch_bitmap_count(const uint32_t *bm, uint64_t nbits, unsigned long long *count, int sm_count,
+                         cudaStream_t s);
+void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count,
+                       int sm_count, cudaStream_t s);
+
+// ---- BinDex on the GPU (bindex.cu) ----
+struct GpuBinDex {
+  int K = 0;
+  uint64_t n = 0;
+  uint32_t *sval = nullptr;   // values in sorted order (n)
+  uint32_t *spos = nullptr;   // row of each sorted value (n)
+  uint32_t *fv = nullptr;     // (K-1) filter vectors of words_for(n) words each
+  uint64_t fv_stride = 0;     // words per filter vector (>= words_for(n), multiple of 4)
+  std::vector<uint32_t> start;      // area start values (K), host copy
+  std::vector<uint64_t> first_rank; // lower_bound of start[k] in sorted order (K), host copy
+  std::vector<uint32_t> sample;     // every kSampleStride-th sorted value, host copy
+  uint32_t min_val = 0, max_val = 0;
+  ~GpuBinDex();
+};
+constexpr int kSampleStride = 1024;
+std::unique_ptr<GpuBinDex> build_bindex(const uint32_t *col, uint64_t n, int K, int sm_count,
+                                        cudaStream_t s);
+// Conjunctive query through the column indexes (all referenced columns
+// must be indexed).  Throws rts::Error.
+void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out, unsigned long long *count,
+                  cudaStream_t s);
+
+// A 256-byte device buffer owned by the context (blocking-call counts).
+unsigned long long *small_device_buffer(rts_ctx *ctx);
+
+}  // namespace rts
+
+// The context.  Defined here so every translation unit sees one layout.
+struct rts_ctx {
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  uint64_t nrows = 0;
+  std::vector<const uint32_t *> cols;
+  uint32_t *owned = nullptr;  // one allocation backing owned columns
+  uint64_t col_stride = 0;    // values between owned columns
+  std::vector<std::unique_ptr<rts::GpuBinDex>> bindex;
+  // scratch for the separate-pass path and the BinDex planner
+  std::vector<uint32_t *> scratch_bm;
+  uint64_t scratch_words = 0;
+  void *plan_dev = nullptr;
+  size_t plan_bytes = 0;
+  void *plan_host = nullptr;  // pinned
+  void *small_dev = nullptr;
+  std::atomic<uint64_t> launches{0};
+  std::string err;
+  ~rts_ctx();
+};

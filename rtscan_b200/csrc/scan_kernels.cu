@@ -1,0 +1,292 @@
+// Fused range-predicate scan kernels for sm_100a.
+//
+// The scan contract is the reference's raw_scan (bindex.cpp:1851-1892)
+// evaluated on every column of a query and ANDed (refine_result_bitmap,
+// bindex.cpp:1259-1281), with the MSB-first bit order of refine()
+// (bindex.cpp:1217) and the hit count of compare_bitmap
+// (bindex.cpp:1959-1978).  The reference computes it with one kernel launch
+// per column and per AND (cuda_and.cu:13-61, 255-296) and counts on the
+// host; here one pass reads each referenced column once and writes the
+// packed words and the count.
+//
+// Work decomposition: a warp owns a tile of 1024 consecutive rows.  For each
+// term every lane issues eight independent 16-byte loads (rows
+// 128k + 4*lane .. +3, k = 0..7), so a warp's load instruction covers 512
+// contiguous bytes and each lane keeps 128 bytes per column in flight.  The
+// per-lane 4-bit hit nibbles are merged into 32 MSB-first words by a
+// three-step reduce-scatter over groups of 8 lanes (7 shuffles per tile), and
+// the warp then stores its 32 words as one 128-byte segment.  The kernel is
+// HBM-bound: 4 bytes per row per column read plus 1/8 byte per row written.
+#include <cuda_runtime.h>
+
+#include "rts_internal.h"
+
+namespace rts {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ uint4 ld_stream(const uint32_t *p) {
+  uint4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ bool in_range(uint32_t x, uint32_t lo, uint32_t span) { return x - lo <= span; }
+
+// Merge the eight per-lane nibbles m[k] (bit 3-j = row 128k+4*lane+j) of a
+// warp into the tile's 32 words; lane (g = lane>>3, q = lane&7) returns word
+// 4q+g of the tile.
+__device__ __forceinline__ uint32_t pack_tile(const uint32_t (&m)[8], int lane) {
+  const int q = lane & 7;
+  const int sh = 28 - 4 * q;
+  uint32_t w[4];
+  const bool a = q & 4;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    uint32_t lo_k = m[i] << sh, hi_k = m[i + 4] << sh;
+    uint32_t send = a ? lo_k : hi_k;
+    uint32_t keep = a ? hi_k : lo_k;
+    w[i] = keep | __shfl_xor_sync(kFull, send, 4);
+  }
+  uint32_t x[2];
+  const bool b = q & 2;
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    uint32_t send = b ? w[i] : w[i + 2];
+    uint32_t keep = b ? w[i + 2] : w[i];
+    x[i] = keep | __shfl_xor_sync(kFull, send, 2);
+  }
+  const bool c = q & 1;
+  uint32_t send = c ? x[0] : x[1];
+  uint32_t keep = c ? x[1] : x[0];
+  return keep | __shfl_xor_sync(kFull, send, 1);
+}
+
+// Evaluate one term on the eight vectors of a tile and AND into m.
+template <bool First>
+__device__ __forceinline__ void eval_term(const DevTerm &t, uint64_t row0, int lane, uint32_t (&m)[8]) {
+  const uint32_t *p = t.col + row0 + 4 * lane;
+  uint4 v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = ld_stream(p + 128 * k);
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    uint32_t nib = (in_range(v[k].x, t.lo, t.span) ? 8u : 0u) | (in_range(v[k].y, t.lo, t.span) ? 4u : 0u) |
+                   (in_range(v[k].z, t.lo, t.span) ? 2u : 0u) | (in_range(v[k].w, t.lo, t.span) ? 1u : 0u);
+    m[k] = First ? nib : (m[k] & nib);
+  }
+}
+
+// Scalar tile: lane handles rows row0 + 32*i + lane, i = 0..31, with bounds
+// checks; used for the last partial tile and for unaligned columns.  Returns
+// word i in lane i.
+__device__ __forceinline__ uint32_t scalar_tile(const ScanParams &p, uint64_t row0, int lane) {
+  uint32_t mine = 0;
+  for (int i = 0; i < 32; i++) {
+    uint64_t row = row0 + 32ull * i + lane;
+    bool hit = row < p.nrows;
+    for (int t = 0; t < p.nterms && hit; t++) hit = in_range(p.t[t].col[row], p.t[t].lo, p.t[t].span);
+    uint32_t bal = __ballot_sync(kFull, hit);
+    if (lane == i) mine = __brev(bal);  // ballot bit j = row 32i+j; MSB-first wants bit 31-j
+  }
+  return mine;
+}
+
+__device__ __forceinline__ void block_count(unsigned long long *count, uint32_t cnt) {
+  __shared__ unsigned long long part[kThreads / 32];
+  cnt = __reduce_add_sync(kFull, cnt);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) part[warp] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < kThreads / 32; i++) s += part[i];
+    if (s) atomicAdd(count, s);
+  }
+}
+
+// NT > 0: exactly NT terms (unrolled); NT == 0: p.nterms terms at run time.
+template <int NT, bool VEC>
+__global__ void __launch_bounds__(kThreads) scan_fused_kernel(const __grid_constant__ ScanParams p) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  const uint64_t nwarps = (uint64_t)gridDim.x * (kThreads / 32);
+  uint32_t cnt = 0;
+  if (VEC) {
+    const int q = lane & 7, g = lane >> 3;
+    for (uint64_t tile = warp; tile < p.full_tiles; tile += nwarps) {
+      const uint64_t row0 = tile * kTileRows;
+      uint32_t m[8];
+      if (NT > 0) {
+        eval_term<true>(p.t[0], row0, lane, m);
+#pragma unroll
+        for (int t = 1; t < NT; t++) eval_term<false>(p.t[t], row0, lane, m);
+      } else {
+        eval_term<true>(p.t[0], row0, lane, m);
+        for (int t = 1; t < p.nterms; t++) eval_term<false>(p.t[t], row0, lane, m);
+      }
+      uint32_t word = pack_tile(m, lane);
+      uint32_t *dst = p.out + tile * kTileWords + 4 * q + g;
+      if (p.and_into) word &= *dst;
+      *dst = word;
+      cnt += __popc(word);
+    }
+  }
+  // Tiles the vector loop did not take: all of them when !VEC, else only
+  // the last partial tile.  Spread over warps the same way.
+  const uint64_t first = VEC ? p.full_tiles : 0;
+  const uint64_t ntiles = (p.nrows + kTileRows - 1) / kTileRows;
+  const uint64_t total_words = (p.nrows + 31) >> 5;
+  for (uint64_t tile = first + warp; tile < ntiles; tile += nwarps) {
+    uint32_t word = scalar_tile(p, tile * kTileRows, lane);
+    uint64_t wi = tile * kTileWords + lane;
+    if (wi < total_words) {
+      if (p.and_into) word &= p.out[wi];
+      p.out[wi] = word;
+      cnt += __popc(word);
+    }
+  }
+  if (p.count) block_count(p.count, cnt);
+}
+
+template <int NT, bool VEC>
+int max_blocks(int sm_count) {
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, scan_fused_kernel<NT, VEC>, kThreads, 0) != cudaSuccess ||
+        b < 1)
+      b = 1;
+    per_sm = b;
+  }
+  return per_sm * sm_count;
+}
+
+template <int NT, bool VEC>
+void launch_nt(const ScanParams &p, int sm_count, cudaStream_t s) {
+  const uint64_t ntiles = (p.nrows + kTileRows - 1) / kTileRows;
+  uint64_t want = (ntiles + (kThreads / 32) - 1) / (kThreads / 32);
+  int blocks = (int)std::min<uint64_t>(want, (uint64_t)max_blocks<NT, VEC>(sm_count));
+  if (blocks < 1) blocks = 1;
+  scan_fused_kernel<NT, VEC><<<blocks, kThreads, 0, s>>>(p);
+}
+
+// ---- bitmap utilities --------------------------------------------------------
+
+__global__ void bitmap_op_kernel(int op, uint32_t *dst, const uint32_t *a, const uint32_t *b, uint64_t words,
+                                 uint32_t value, int vec) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  auto f = [&](uint32_t x, uint32_t y) -> uint32_t {
+    switch (op) {
+      case RTS_BM_AND: return x & y;
+      case RTS_BM_OR: return x | y;
+      case RTS_BM_COPY: return x;
+      case RTS_BM_NOT: return ~x;
+      case RTS_BM_ANDNOT: return y & ~x;
+      default: return value;
+    }
+  };
+  uint64_t done = 0;
+  if (vec) {
+    const uint64_t nv = words / 4;
+    for (uint64_t i = tid; i < nv; i += stride) {
+      uint4 x = op == RTS_BM_FILL ? make_uint4(0, 0, 0, 0) : reinterpret_cast<const uint4 *>(a)[i];
+      uint4 y = (op == RTS_BM_AND || op == RTS_BM_OR || op == RTS_BM_ANDNOT) ? reinterpret_cast<const uint4 *>(b)[i]
+                                                                             : make_uint4(0, 0, 0, 0);
+      reinterpret_cast<uint4 *>(dst)[i] = make_uint4(f(x.x, y.x), f(x.y, y.y), f(x.z, y.z), f(x.w, y.w));
+    }
+    done = nv * 4;
+  }
+  for (uint64_t i = done + tid; i < words; i += stride) {
+    uint32_t x = op == RTS_BM_FILL ? 0u : a[i];
+    uint32_t y = (op == RTS_BM_AND || op == RTS_BM_OR || op == RTS_BM_ANDNOT) ? b[i] : 0u;
+    dst[i] = f(x, y);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) bitmap_count_kernel(const uint32_t *bm, uint64_t nbits, int vec,
+                                                                 unsigned long long *count) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t full = nbits >> 5;
+  uint32_t cnt = 0;
+  uint64_t done = 0;
+  if (vec) {
+    const uint64_t nv = full / 4;
+    for (uint64_t i = tid; i < nv; i += stride) {
+      uint4 x = reinterpret_cast<const uint4 *>(bm)[i];
+      cnt += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+    }
+    done = nv * 4;
+  }
+  for (uint64_t i = done + tid; i < full; i += stride) cnt += __popc(bm[i]);
+  const uint32_t rem = (uint32_t)(nbits & 31);
+  if (rem && tid == 0) cnt += __popc(bm[full] & ~(0xFFFFFFFFu >> rem));
+  block_count(count, cnt);
+}
+
+__global__ void fill_range_kernel(uint32_t *out, uint64_t nrows, uint32_t ones) {
+  const uint64_t words = (nrows + 31) >> 5;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t rem = (uint32_t)(nrows & 31);
+  for (uint64_t i = tid; i < words; i += stride) {
+    uint32_t w = ones ? 0xFFFFFFFFu : 0u;
+    if (rem && i == words - 1) w &= ~(0xFFFFFFFFu >> rem);
+    out[i] = w;
+  }
+}
+
+__global__ void store_count_kernel(unsigned long long *count, unsigned long long v) { *count = v; }
+
+int grid_for(uint64_t items, int per_thread, int sm_count) {
+  uint64_t threads = (items + per_thread - 1) / per_thread;
+  uint64_t blocks = (threads + kThreads - 1) / kThreads;
+  uint64_t cap = (uint64_t)sm_count * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+}  // namespace
+
+void launch_scan_fused(const ScanParams &p, bool vector_ok, int sm_count, cudaStream_t s) {
+  if (vector_ok) {
+    switch (p.nterms) {
+      case 1: launch_nt<1, true>(p, sm_count, s); break;
+      case 2: launch_nt<2, true>(p, sm_count, s); break;
+      case 3: launch_nt<3, true>(p, sm_count, s); break;
+      case 4: launch_nt<4, true>(p, sm_count, s); break;
+      default: launch_nt<0, true>(p, sm_count, s); break;
+    }
+  } else {
+    launch_nt<0, false>(p, sm_count, s);
+  }
+}
+
+void launch_bitmap_op(int op, uint32_t *dst, const uint32_t *a, const uint32_t *b, uint64_t words,
+                      uint32_t value, int sm_count, cudaStream_t s) {
+  bool vec = (((uintptr_t)dst | (uintptr_t)(a ? a : dst) | (uintptr_t)(b ? b : dst)) & 15) == 0;
+  bitmap_op_kernel<<<grid_for(words, 16, sm_count), kThreads, 0, s>>>(op, dst, a, b, words, value, vec ? 1 : 0);
+}
+
+void launch_bitmap_count(const uint32_t *bm, uint64_t nbits, unsigned long long *count, int sm_count,
+                         cudaStream_t s) {
+  bool vec = ((uintptr_t)bm & 15) == 0;
+  bitmap_count_kernel<<<grid_for(nbits >> 5, 16, sm_count), kThreads, 0, s>>>(bm, nbits, vec ? 1 : 0, count);
+}
+
+void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count, int sm_count,
+                       cudaStream_t s) {
+  uint64_t words = (nrows + 31) >> 5;
+  if (words) fill_range_kernel<<<grid_for(words, 4, sm_count), kThreads, 0, s>>>(out, nrows, ones ? 1u : 0u);
+  if (count) store_count_kernel<<<1, 1, 0, s>>>(count, ones ? (unsigned long long)nrows : 0ull);
+}
+
+}  // namespace rts

@@ -1,0 +1,107 @@
+"""GPU BinDex: index contents against the oracle's restated BinDex, and
+query results (sieve mode and candidate mode) against the scalar filter."""
+import numpy as np
+import pytest
+
+import rtscan_b200 as R
+from oracle import oracle as O
+from rtscan_b200 import datagen as D
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+KINDS = ["uniform", "uniform2p6", "uniform2p8", "zipf1.1", "zipf1.5", "normal"]
+
+
+def bindex_scan(ctx, terms):
+    n = ctx.nrows
+    bm = torch.full((R.bitmap_words(n),), -1, dtype=torch.int32, device="cuda")
+    cnt = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+    ctx.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return bm.cpu().numpy().view(np.uint32), int(cnt.item())
+
+
+def expect(cols, terms):
+    n = len(cols[0])
+    if any(lo > hi for _, lo, hi in terms):
+        return np.zeros(O.words(n), np.uint32), 0
+    if not terms:
+        return O.mask_tail(np.full(O.words(n), 0xFFFFFFFF, np.uint32), n), n
+    return O.range_scan([cols[c] for c, _, _ in terms], [t[1] for t in terms], [t[2] for t in terms])
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("K", [8, 128])
+def test_index_matches_restated_bindex(ctx, kind, K):
+    n = 300_007
+    col = D.column(kind, n, 3)
+    ctx.load_columns([col])
+    ctx.build_bindex(0, K)
+    ob = O.BinDex(col, K=K)
+    starts, ranks = ctx.bindex_areas(0, K)
+    assert np.array_equal(starts, ob.area_start_values())
+    s = np.sort(col)
+    assert np.array_equal(ranks, np.searchsorted(s, starts, side="left").astype(np.uint64))
+    for k in sorted({0, 1, K // 2, K - 2}):
+        assert np.array_equal(ctx.bindex_filter_vector(0, k), ob.filter_vector(k)), k
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_single_column_queries(ctx, kind):
+    n = (1 << 20) + 13
+    col = D.column(kind, n, 11)
+    ctx.load_columns([col])
+    ctx.build_bindex(0, 128)
+    s = np.sort(col)
+    rng = np.random.default_rng(2)
+    cases = [(0, 0), (0, 0xFFFFFFFE), (1, 0xFFFFFFFF), (int(s[0]), int(s[0])), (int(s[-1]), 0xFFFFFFFF),
+             (int(s[n // 2]), int(s[n // 2])), (5, 4)]
+    for _ in range(25):
+        i, j = sorted(rng.integers(0, n, size=2).tolist())
+        cases.append((int(s[i]), int(s[j])))
+        cases.append((int(s[i]), int(s[i]) + int(rng.integers(0, 3))))  # tight: candidate mode
+    for lo, hi in cases:
+        got, cnt = bindex_scan(ctx, [(0, lo, hi)])
+        want, wcnt = expect([col], [(0, lo, hi)])
+        assert cnt == wcnt, (kind, lo, hi, cnt, wcnt)
+        assert np.array_equal(got, want), (kind, lo, hi)
+
+
+@pytest.mark.parametrize("ncols", [2, 3, 4])
+def test_conjunctive_queries(ctx, ncols):
+    n = 500_003
+    kinds = ["uniform", "zipf1.3", "uniform2p8", "normal"][:ncols]
+    cols = [D.column(k, n, 40 + i) for i, k in enumerate(kinds)]
+    ctx.load_columns(cols)
+    for c in range(ncols):
+        ctx.build_bindex(c, 128)
+    qs = D.batch_queries(cols, 40, seed=ncols, min_sel=1e-4, max_sel=0.9, min_cols=1, max_cols=ncols)
+    for q in qs:
+        got, cnt = bindex_scan(ctx, q)
+        want, wcnt = expect(cols, q)
+        assert cnt == wcnt, (q, cnt, wcnt)
+        assert np.array_equal(got, want), q
+
+
+def test_missing_index_is_an_error(ctx):
+    n = 10_000
+    ctx.load_columns([D.uniform(n, 1), D.uniform(n, 2)])
+    ctx.build_bindex(0, 16)
+    with pytest.raises(R.RtsError) as e:
+        bindex_scan(ctx, [(0, 1, 2), (1, 3, 4)])
+    assert e.value.code == -6
+    with pytest.raises(R.RtsError):
+        ctx.build_bindex(1, 1)
+
+
+def test_blocking_scan_uses_index(ctx):
+    n = 200_000
+    cols = [D.uniform(n, 5), D.zipf(n, 6, 1.1)]
+    ctx.load_columns(cols)
+    ctx.build_bindex(0, 64)
+    ctx.build_bindex(1, 64)
+    q = [(0, 1 << 30, 1 << 31), (1, 0, 3)]
+    bm, cnt = ctx.scan(q)
+    want, wcnt = expect(cols, q)
+    assert cnt == wcnt and np.array_equal(bm, want)
