@@ -1,13 +1,15 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batched|single|multi] [--nrows N]
+                    [--workload batched|single|multi] [--nrows N] [--queries Q]
 
-Workloads (seeded synthetic data on the device; no dataset is read):
-  batched  1e8 rows x 4 uint32 columns (zipf 1.1, 1.3, 1.5 over 2^20
-           values and a rounded normal), 1024 queries touching 1-4 columns
-           with log-uniform selectivity in [0.01%, 90%]; one step = one
-           batched pass answering all queries (bitmaps + counts).
+Workloads (seeded synthetic data generated on the device; no dataset is read):
+  batched  (default) 1e8 rows x 4 uint32 columns (zipf 1.1, 1.3, 1.5 over 2^20
+           values and a rounded normal, mean 2^31, sd 2^28), 1024 queries
+           touching 1-4 columns with log-uniform selectivity in [0.01%, 90%];
+           one step = one batched call answering all queries (1024 bitmaps
+           + counts).  Compared with one fused-scan launch per query, and at
+           256 concurrent 4-column queries.
   single   1e8 rows x 1 uniform column, one 10%-selectivity range; one step
            = one fused scan launch.
   multi    1e8 rows x 4 uniform columns, one conjunctive query with
@@ -16,13 +18,13 @@ Workloads (seeded synthetic data on the device; no dataset is read):
 Under torchrun each rank scans its own rows (weak scaling, no collective on
 the data path); `value` is the aggregate over ranks.  Timing: W warm-up
 steps, then K steps between CUDA events on the launching stream, barrier +
-synchronize on both sides, max over ranks.  Inputs are larger than L2.
+synchronize on both sides, max over ranks.  Inputs are larger than L2
+(400 MB per column).
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -37,6 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "batched range-scan GB/s & queries/s vs HBM peak; served query p50/p99 ms"
+BATCH_KINDS = ["zipf1.1", "zipf1.3", "zipf1.5", "normal"]
 
 
 # ----------------------------------------------------------------------------
@@ -44,10 +47,8 @@ METRIC = "batched range-scan GB/s & queries/s vs HBM peak; served query p50/p99 
 # ----------------------------------------------------------------------------
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
 
 
 def peaks():
@@ -116,7 +117,7 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------
-# synthetic columns on the device
+# synthetic columns on the device (same distributions as rtscan_b200.datagen)
 # ----------------------------------------------------------------------------
 
 def gpu_column(torch, kind: str, n: int, seed: int, device):
@@ -125,22 +126,20 @@ def gpu_column(torch, kind: str, n: int, seed: int, device):
     if kind == "uniform":
         x = torch.randint(0, 1 << 32, (n,), generator=g, device=device, dtype=torch.int64)
         return x.to(torch.int32)  # two's-complement wrap keeps the uint32 bit pattern
+    out = torch.empty(n, dtype=torch.int32, device=device)
+    chunk = 1 << 24
     if kind.startswith("zipf"):
         s = float(kind[4:])
         distinct = 1 << 20
         ranks = torch.arange(1, distinct + 1, device=device, dtype=torch.float64)
         cdf = torch.cumsum(ranks.pow(-s), 0)
         cdf /= cdf[-1].clone()
-        out = torch.empty(n, dtype=torch.int32, device=device)
-        chunk = 1 << 24
         for i in range(0, n, chunk):
             m = min(chunk, n - i)
             u = torch.rand(m, generator=g, device=device, dtype=torch.float64)
             out[i:i + m] = torch.clamp(torch.searchsorted(cdf, u, right=True), max=distinct - 1).to(torch.int32)
         return out
     if kind == "normal":
-        out = torch.empty(n, dtype=torch.int32, device=device)
-        chunk = 1 << 24
         for i in range(0, n, chunk):
             m = min(chunk, n - i)
             x = torch.randn(m, generator=g, device=device, dtype=torch.float64) * (2.0 ** 28) + 2.0 ** 31
@@ -149,16 +148,36 @@ def gpu_column(torch, kind: str, n: int, seed: int, device):
     raise ValueError(kind)
 
 
-def host_sample(torch, col, m=1 << 20, seed=0):
+def host_sample(torch, col, m=1 << 18, seed=0):
     g = torch.Generator(device=col.device)
     g.manual_seed(seed)
     idx = torch.randint(0, col.numel(), (m,), generator=g, device=col.device)
     return np.sort(col[idx].cpu().numpy().view(np.uint32))
 
 
+def make_queries(D, wl, samples, nq, seed=42):
+    rng = np.random.default_rng(seed)
+    if wl == "single":
+        return [[(0, *D.range_for_selectivity(samples[0], 0.10))]]
+    if wl == "multi":
+        q = []
+        for c in range(len(samples)):
+            sel = rng.uniform(0.05, 0.5)
+            q.append((c, *D.range_for_selectivity(samples[c], sel, rng.uniform(sel / 2, 1 - sel / 2))))
+        return [q]
+    return D.batch_queries(samples, nq, seed=seed)
+
+
+def step_bytes(n, queries):
+    """Algorithmic bytes of one step: every referenced column read once plus
+    one bitmap written per query."""
+    used = {c for q in queries for c, _, _ in q}
+    return 4 * n * len(used) + len(queries) * n / 8
+
+
 # ----------------------------------------------------------------------------
-# CPU baseline: the reference's own CPU BinDex (oracle/_ref) when it was
-# built, else the oracle's C restatement; timed on this host.
+# CPU baseline: the reference's own CPU BinDex (oracle/_ref, compiled from
+# the reference sources) when present, else the oracle's C restatement.
 # ----------------------------------------------------------------------------
 
 REF_N = 1 << 24
@@ -170,8 +189,8 @@ def reference_binary():
 
 
 def cpu_reference_run(cols_np, queries, repeats=3, max_seconds=60.0):
-    """Time the reference BinDex query loop (build excluded) on a sample of
-    REF_N rows; returns (seconds per query, kind, cores, detail)."""
+    """Time the reference BinDex query loop (index build excluded) on
+    REF_N-row columns; returns (seconds per query, kind, cores, detail)."""
     from rtscan_b200 import datagen as D
     ncols = len(cols_np)
     binary = reference_binary()
@@ -184,14 +203,14 @@ def cpu_reference_run(cols_np, queries, repeats=3, max_seconds=60.0):
                 f.write(D.to_scan_cmd(queries, ncols))
             t0 = time.time()
             r = subprocess.run([binary, "-f", data, "-b", str(ncols), "-p", cmdf, "-r", str(repeats)],
-                               capture_output=True, text=True, timeout=max_seconds + 240)
+                               capture_output=True, text=True, timeout=max_seconds + 300)
             if r.returncode != 0:
                 raise RuntimeError("reference harness failed: " + r.stderr[-500:])
-            ms = [float(l.split()[-1]) for l in r.stdout.splitlines() if l.startswith("query ")]
-            eq = [l.split()[8] == "1" for l in r.stdout.splitlines() if l.startswith("query ")]
+            q = [l.split() for l in r.stdout.splitlines() if l.startswith("query ")]
+            ms = [float(x[-1]) for x in q]
             return (sum(ms) / 1e3 / len(ms), "reference", 20,
-                    {"queries": len(ms), "all_equal_scalar": all(eq), "wall_s": round(time.time() - t0, 1)})
-    # fall back to the restated scalar filter (single thread)
+                    {"queries": len(ms), "reference_bindex_equals_scalar": all(x[7] == "1" for x in q),
+                     "wall_s": round(time.time() - t0, 1)})
     from oracle import oracle as O
     t0 = time.time()
     done = 0
@@ -203,8 +222,13 @@ def cpu_reference_run(cols_np, queries, repeats=3, max_seconds=60.0):
     return (time.time() - t0) / done, "port", 1, {"queries": done}
 
 
+def cpu_sample_columns(kinds, m):
+    from rtscan_b200 import datagen as D
+    return [D.column(k, m, 1000 + i) for i, k in enumerate(kinds)]
+
+
 # ----------------------------------------------------------------------------
-# workloads
+# our arm
 # ----------------------------------------------------------------------------
 
 def run(args):
@@ -216,7 +240,8 @@ def run(args):
 
     world, rank, local = dist_env()
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = R.Context(local)
@@ -226,39 +251,21 @@ def run(args):
 
     n = args.nrows
     wl = args.workload
-    if wl == "single":
-        kinds = ["uniform"]
-    elif wl == "multi":
-        kinds = ["uniform"] * 4
-    else:
-        kinds = ["zipf1.1", "zipf1.3", "zipf1.5", "normal"]
+    kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, BATCH_KINDS)
     cols = [gpu_column(torch, k, n, 1000 * (rank + 1) + i, dev) for i, k in enumerate(kinds)]
     ctx.attach_columns([c.data_ptr() for c in cols], n)
     samples = [host_sample(torch, c, seed=7 + i) for i, c in enumerate(cols)]
+    queries = make_queries(D, wl, samples, args.queries)
+    pq = R.prepare(queries)
+    nq = len(queries)
     words = R.bitmap_words(n)
     stride = (words + 31) // 32 * 32
-
-    rng = np.random.default_rng(42)
-    if wl == "single":
-        queries = [[(0, *D.range_for_selectivity(samples[0], 0.10))]]
-    elif wl == "multi":
-        q = []
-        for c in range(4):
-            sel = rng.uniform(0.05, 0.5)
-            q.append((c, *D.range_for_selectivity(samples[c], sel, rng.uniform(sel / 2, 1 - sel / 2))))
-        queries = [q]
-    else:
-        queries = D.batch_queries([s_ for s_ in samples], args.queries, seed=42)  # sample-based bounds
-    nq = len(queries)
     out = torch.empty(nq * stride, dtype=torch.int32, device=dev)
     cnt = torch.zeros(nq, dtype=torch.int64, device=dev)
-
-    used_cols = sorted({c for q in queries for c, _, _ in q})
+    bytes_step = step_bytes(n, queries)
     if wl == "batched":
-        bytes_step = 4 * n * len(used_cols) + nq * n / 8
-        launch = lambda: ctx.scan_batch_async(queries, out.data_ptr(), stride, cnt.data_ptr(), s)
+        launch = lambda: ctx.scan_batch_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s)
     else:
-        bytes_step = 4 * n * len(used_cols) + n / 8
         launch = lambda: ctx.scan_async(queries[0], out.data_ptr(), cnt.data_ptr(), s)
 
     def barrier():
@@ -266,65 +273,88 @@ def run(args):
         if world > 1:
             dist.barrier()
 
+    def timed(fn, steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for i in range(steps):
+            fn()
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        return [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)], ev[0].elapsed_time(ev[-1])
+
     for _ in range(args.warmup):
         launch()
     barrier()
-    l0 = ctx.launches
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    l0 = ctx.launches
     barrier()
-    ev[0].record(stream)
-    for i in range(args.steps):
-        launch()
-        ev[i + 1].record(stream)
+    per, total_ms = timed(launch, args.steps)
     barrier()
-    clk = clocks.stop()
     launches = ctx.launches - l0
-    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
+    clk = clocks.stop()
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_step = float(t.item()) / args.steps
+    kern_launches = max(1, launches // args.steps)
+    ms_launch = statistics.median(per) / kern_launches
+    achieved = (bytes_step / kern_launches) / (ms_launch * 1e-3) / 1e9
 
-    # dominant kernel: the step is one launch of it on this stream
-    kern_ms = statistics.median(per)
-    achieved = bytes_step / (kern_ms * 1e-3) / 1e9
-
-    # comparisons on rank 0's device
     extra = {}
     if wl == "multi":
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for _ in range(3):
             ctx.scan_separate_async(queries[0], out.data_ptr(), cnt.data_ptr(), s)
-        e0.record(stream)
-        for _ in range(args.steps):
-            ctx.scan_separate_async(queries[0], out.data_ptr(), cnt.data_ptr(), s)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        sep_ms = e0.elapsed_time(e1) / args.steps
+        per_sep, _ = timed(lambda: ctx.scan_separate_async(queries[0], out.data_ptr(), cnt.data_ptr(), s), args.steps)
+        sep_ms = statistics.median(per_sep)
         extra["separate_passes_ms"] = round(sep_ms, 4)
-        extra["fused_speedup_vs_separate"] = round(sep_ms / ms_step, 3)
+        extra["fused_speedup_vs_separate"] = round(sep_ms / statistics.median(per), 3)
+    if wl == "batched" and not args.no_compare:
+        each = lambda: ctx.scan_each_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s)
+        each()
+        per_each, _ = timed(each, 2)
+        each_ms = statistics.median(per_each)
+        extra["one_query_per_launch_ms"] = round(each_ms, 3)
+        extra["batched_speedup_vs_one_per_launch"] = round(each_ms / statistics.median(per), 2)
+        # north-star comparison: 256 concurrent 4-column queries
+        q4 = D.batch_queries(samples, 256, seed=7, min_cols=4, max_cols=4)
+        pq4 = R.prepare(q4)
+        b4 = lambda: ctx.scan_batch_async(pq4, out.data_ptr(), stride, cnt.data_ptr(), s)
+        e4 = lambda: ctx.scan_each_async(pq4, out.data_ptr(), stride, cnt.data_ptr(), s)
+        b4(); e4()
+        pb4, _ = timed(b4, 3)
+        pe4, _ = timed(e4, 2)
+        mb4, me4 = statistics.median(pb4), statistics.median(pe4)
+        extra["q256x4col"] = {"batched_ms": round(mb4, 3), "one_per_launch_ms": round(me4, 3),
+                              "batched_qps": round(256 / (mb4 * 1e-3), 1),
+                              "one_per_launch_qps": round(256 / (me4 * 1e-3), 1),
+                              "speedup": round(me4 / mb4, 2)}
 
-    # e2e through the C-ABI with host buffers: columns uploaded from pinned
-    # host memory and the result bitmap read back, every step.
-    e2e_s = float("nan")
+    # e2e through the C-ABI with host buffers: the step's columns uploaded
+    # from pinned host memory and every result bitmap + count read back.
+    e2e = None
     if not args.no_e2e:
         host_cols = [c.cpu().pin_memory() for c in cols]
         host_np = [h.numpy().view(np.uint32) for h in host_cols]
-        e2e_steps = max(2, min(args.steps, 5))
+        hb = torch.empty((nq, stride), dtype=torch.int32).pin_memory()
+        hb_np = hb.numpy().view(np.uint32)
+        ctx.scan_batch_host(host_np, pq, hb_np, stride)  # warm-up (allocates device buffers)
+        reps = 2 if wl == "batched" else 5
         barrier()
         t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            ctx.load_columns(host_np)
-            for q in queries[: (1 if wl != "batched" else nq)]:
-                ctx.scan(q)
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
-        ctx.attach_columns([c.data_ptr() for c in cols], n)
-    h2d = 4 * n * len(cols)
-    d2h = (nq if wl == "batched" else 1) * (words * 4 + 8)
+        for _ in range(reps):
+            _, counts = ctx.scan_batch_host(host_np, pq, hb_np, stride)
+        e2e_s = (time.perf_counter() - t0) / reps
+        et = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e_s = float(et.item())
+        e2e = {"value": round(bytes_step * world / e2e_s / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": int(4 * n * len(cols)), "d2h_bytes_per_step": int(nq * (stride * 4 + 8)),
+               "queries_per_s": round(nq * world / e2e_s, 2), "ms_per_step": round(e2e_s * 1e3, 2),
+               "api": "rts_scan_batch_host"}
+        del hb, host_cols
 
     gbs_total = bytes_step * world / (ms_step * 1e-3) / 1e9
     line = {
@@ -340,31 +370,33 @@ def run(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded, generated on device)",
-        "config": {"workload": {"batched": "batched 1e8x4 skewed, 1024 queries", "single": "single-column 1e8 scan 10%",
-                                "multi": "multi-column 1e8x4 conjunctive"}[wl],
-                   "nrows_per_gpu": n, "ncols": len(cols), "queries_per_step": nq, "l2": "inputs larger than L2"},
+        "config": {"workload": {"batched": f"batched scan 1e8 rows x 4 skewed columns, {nq} queries",
+                                "single": "single-column 1e8-row scan, 10% selectivity",
+                                "multi": "4-column 1e8-row conjunctive scan"}[wl],
+                   "nrows_per_gpu": n, "ncols": len(cols), "queries_per_step": nq,
+                   "column_kinds": kinds, "l2": "inputs larger than L2 (400 MB per column)"},
         "queries_per_s": round(nq * world / (ms_step * 1e-3), 1),
         "rows_per_s": round(n * world / (ms_step * 1e-3), 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind},
-        "e2e": {"value": round(bytes_step / e2e_s / 1e9 * world, 3), "unit": "GB/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "queries_per_s": round((nq if wl == 'batched' else 1) * world / e2e_s, 2)},
+                     "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                     "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel_launches_per_step": kern_launches},
+        "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk,
     }
     line.update(extra)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        m = REF_N
-        cols_np = [c[:m].cpu().numpy().view(np.uint32).copy() for c in cols]
-        qs = queries[: min(len(queries), 8)]
+        cols_np = cpu_sample_columns(kinds, REF_N)
+        smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols_np]
+        qs = make_queries(D, wl, smp, args.queries)[: 16]
         sec, kind, cores, detail = cpu_reference_run(cols_np, qs)
-        used = len({c for q in qs for c, _, _ in q})
-        cpu_bytes = 4 * m * used / len(qs) * 0 + sum(4 * m * len({c for c, _, _ in q}) + m / 8 for q in qs) / len(qs)
-        line["cpu_baseline"] = {"value": round(cpu_bytes / sec / 1e9, 3), "unit": "GB/s", "cores": cores,
-                                "kind": kind, "queries_per_s": round(1.0 / sec, 2),
-                                "sample": f"{m} rows x {len(cols)} cols, {len(qs)} queries of this workload",
+        b = sum(step_bytes(REF_N, [q]) for q in qs) / len(qs)
+        line["cpu_baseline"] = {"value": round(b / sec / 1e9, 3), "unit": "GB/s", "cores": cores, "kind": kind,
+                                "queries_per_s": round(1.0 / sec, 2),
+                                "sample": f"{REF_N} rows x {len(cols_np)} columns, {len(qs)} queries of this workload "
+                                          "(reference BinDex query loop, index build excluded)",
                                 **detail}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -374,35 +406,26 @@ def run(args):
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU path on this host (rank 0 only)."""
-    world, rank, local = dist_env()
+    """--impl reference: the reference's CPU path on this host, rank 0 only."""
+    world, rank, _ = dist_env()
     if rank != 0:
         return
-    import torch
-
     from rtscan_b200 import datagen as D
-    m = REF_N
     wl = args.workload
-    kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, ["zipf1.1", "zipf1.3", "zipf1.5", "normal"])
-    cols = [D.column(k, m, 1000 + i) for i, k in enumerate(kinds)]
-    samples = [np.sort(c[np.random.default_rng(7).integers(0, m, size=1 << 18)]) for c in cols]
-    rng = np.random.default_rng(42)
-    if wl == "single":
-        queries = [[(0, *D.range_for_selectivity(samples[0], 0.10))]]
-    elif wl == "multi":
-        queries = [[(c, *D.range_for_selectivity(samples[c], 0.2)) for c in range(4)]]
-    else:
-        queries = D.batch_queries(samples, 1024, seed=42)
+    kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, BATCH_KINDS)
+    cols = cpu_sample_columns(kinds, REF_N)
+    smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols]
+    queries = make_queries(D, wl, smp, args.queries)
     per_step = min(len(queries), 8)
-    vals = []
-    kind = cores = None
+    vals, kind, cores, detail = [], None, None, {}
+    t_start = time.time()
     for step in range(args.warmup + args.steps):
         qs = [queries[(step * per_step + i) % len(queries)] for i in range(per_step)]
         sec, kind, cores, detail = cpu_reference_run(cols, qs, repeats=1)
         if step >= args.warmup:
-            b = sum(4 * m * len({c for c, _, _ in q}) + m / 8 for q in qs) / len(qs)
-            vals.append((b / sec / 1e9, 1.0 / sec, sec))
-        if step >= args.warmup + 1 and sum(v[2] for v in vals) * per_step > 120:
+            b = sum(step_bytes(REF_N, [q]) for q in qs) / len(qs)
+            vals.append((b / sec / 1e9, 1.0 / sec))
+        if step >= args.warmup and time.time() - t_start > 150:
             break
     v = statistics.median(x[0] for x in vals)
     qps = statistics.median(x[1] for x in vals)
@@ -410,10 +433,12 @@ def run_reference(args):
             "steps": len(vals), "warmup": args.warmup, "ms_per_step": round(1e3 * per_step / qps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)",
-            "config": {"workload": wl, "nrows": m, "ncols": len(cols), "queries_per_step": per_step},
+            "config": {"workload": wl, "nrows": REF_N, "ncols": len(cols), "queries_per_step": per_step,
+                       "column_kinds": kinds},
             "queries_per_s": round(qps, 2),
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "kind": kind, "cores": cores,
-                             "sample": f"{m} rows x {len(cols)} cols, {per_step} queries per step"},
+                             "sample": f"{REF_N} rows x {len(cols)} columns, {per_step} queries per step "
+                                       "(reference BinDex query loop, index build excluded)", **detail},
             "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -421,17 +446,17 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched", choices=["batched", "single", "multi"])
     ap.add_argument("--nrows", type=int, default=100_000_000)
     ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the one-query-per-launch comparison")
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -218,6 +218,17 @@ RTS_API rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, in
 RTS_API rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
                                         int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
                                         uint64_t *dev_counts, void *stream);
+/* Batched scan over host-resident columns into host bitmaps: uploads the
+ * `ncols` columns of `nrows` values (pinned host memory is fastest), runs
+ * the batched passes, and copies every query's bitmap (host_bitmaps +
+ * q*stride_words) and count (host_counts[q]) back, the download of each
+ * group of queries overlapping the next group's pass.  Blocking.  The
+ * context's resident table is left as it was.  (The reference's per-query
+ * upload-scan-download loop, bindex_cuda.cpp:1771-1946.) */
+RTS_API rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
+                                       uint64_t nrows, const rts_term *terms, const int32_t *offsets,
+                                       int32_t nqueries, uint32_t *host_bitmaps, uint64_t stride_words,
+                                       uint64_t *host_counts);
 /* The same queries with one fused-scan launch per query (the baseline the
  * batched kernel is measured against). */
 RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,

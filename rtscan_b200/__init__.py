@@ -88,6 +88,9 @@ _SIGS = [
                                               ctypes.c_uint64, _P, _P]),
     ("rts_scan_each_async", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P,
                                              ctypes.c_uint64, _P, _P]),
+    ("rts_scan_batch_host", ctypes.c_int32, [_P, ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64, _TERMP,
+                                             ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P, ctypes.c_uint64,
+                                             _P]),
 ]
 
 
@@ -182,6 +185,31 @@ def parse_scan_cmd(text: str, ncols: int) -> QuerySet:
     return QuerySet(text, ncols)
 
 
+class PreparedQueries:
+    """Queries packed once into the C-ABI's CSR arrays (terms + offsets), so
+    repeated batch calls skip the Python-side packing."""
+
+    def __init__(self, queries):
+        flat = []
+        offs = [0]
+        for q in queries:
+            flat.extend(q)
+            offs.append(len(flat))
+        self.terms, _ = make_terms(flat)
+        self.offsets = (ctypes.c_int32 * len(offs))(*offs)
+        self.n = len(queries)
+
+    def csr(self):
+        return self.terms, self.offsets
+
+    def __len__(self):
+        return self.n
+
+
+def prepare(queries) -> PreparedQueries:
+    return PreparedQueries(queries)
+
+
 class Context:
     """A device context with resident columns (rts_ctx)."""
 
@@ -272,14 +300,9 @@ class Context:
 
     @staticmethod
     def _csr(queries):
-        flat = []
-        offs = [0]
-        for q in queries:
-            flat.extend(q)
-            offs.append(len(flat))
-        arr, _ = make_terms(flat)
-        off = (ctypes.c_int32 * len(offs))(*offs)
-        return arr, off
+        if isinstance(queries, PreparedQueries):
+            return queries.terms, queries.offsets
+        return PreparedQueries(queries).csr()
 
     def scan_batch_async(self, queries, bitmaps_ptr: int, stride_words: int, counts_ptr: int, stream: int = 0):
         arr, off = self._csr(queries)
@@ -290,6 +313,22 @@ class Context:
         arr, off = self._csr(queries)
         self._c(lib().rts_scan_each_async(self._h, arr, off, len(queries), bitmaps_ptr, stride_words, counts_ptr,
                                           stream))
+
+    def scan_batch_host(self, host_cols, queries, host_bitmaps=None, stride_words: int = 0):
+        """Host columns (numpy uint32, ideally pinned) in, host bitmaps out.
+        Returns (bitmaps [nq, stride] uint32, counts [nq] uint64)."""
+        import numpy as np
+        n = len(host_cols[0])
+        words = bitmap_words(n)
+        stride = stride_words or words
+        arr, off = self._csr(queries)
+        if host_bitmaps is None:
+            host_bitmaps = np.zeros((len(queries), stride), dtype=np.uint32)
+        counts = np.zeros(len(queries), dtype=np.uint64)
+        ptrs = (_P * len(host_cols))(*[c.ctypes.data for c in host_cols])
+        self._c(lib().rts_scan_batch_host(self._h, ptrs, len(host_cols), n, arr, off, len(queries),
+                                          host_bitmaps.ctypes.data, stride, counts.ctypes.data))
+        return host_bitmaps, counts
 
     def bitmap_op_async(self, op: int, dst: int, a: int, b: int, words: int, value: int = 0, stream: int = 0):
         self._c(lib().rts_bitmap_op_async(self._h, op, dst, a, b, words, value, stream))

@@ -1,0 +1,812 @@
+// Batched scan: many queries in one pass over the columns.
+//
+// The reference answers one query per loop iteration and re-reads its
+// columns every time (bindex_cuda.cpp:1827-1986).  Here a batch is answered
+// by persistent kernels that stream each column chunk from HBM once per
+// pass and evaluate up to 256 queries on it without per-query compares:
+//
+//   * Per pass and column, the host collects the query bounds on that
+//     column (lo and hi+1 of every term) into a sorted boundary list B.  The
+//     boundaries cut the value domain into intervals, and every query's
+//     verdict on the column is constant over an interval.  The kernel finds a
+//     row's interval ("position", #boundaries <= x) with a bucket index plus
+//     a short binary search, both in shared memory.
+//   * A mask table gives, per position, one bit per query (256 bits = eight
+//     32-bit words, one per group of 32 queries).  A row's verdict for all
+//     queries is the AND of its columns' table rows: C shared-memory loads
+//     per row and group instead of up to 2*C compares per row and query.
+//   * Lane (s, g) of a warp owns rows s*8..s*8+7 of a 32-row tile for query
+//     group g.  Its eight 32-bit masks are bit-transposed in registers (three
+//     delta-swap stages) into bytes, the four lanes of a group exchange
+//     bytes so that each finalizes 8 queries' 32-row words, and the words
+//     are staged in shared memory (a rotated layout that is bank-conflict
+//     free on both sides) until eight tiles make a full 32-byte sector per
+//     query, which the warp then stores with coalesced writes.
+//   * Counts are kept per lane in registers and flushed once per CTA.
+// Queries with an empty term, with no constrained column, or with more than
+// eight constrained columns are answered outside this kernel (fill or fused
+// scan), so the result of every query equals the single-query path.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <vector>
+
+#include "rts_internal.h"
+
+namespace rts {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kSlots = 256;         // queries per pass
+constexpr int kGroups = kSlots / 32;
+constexpr int kMaxCols = 8;         // constrained columns per pass
+constexpr int kTilesPerBlock = 8;   // 8 tiles x 32 rows = one 32-byte sector per query
+constexpr int kWarps = 16;
+constexpr int kThreads = kWarps * 32;
+constexpr int kStageWords = kSlots * kTilesPerBlock;  // per warp
+template <int CMAX>
+constexpr int kPosWords = 36 * CMAX;  // per warp: 32 rows + one padding row per 8
+
+struct BatchPass {
+  const uint32_t *col[kMaxCols];
+  uint32_t m[kMaxCols];         // boundaries of column c
+  uint32_t bmin[kMaxCols];      // B[0]
+  uint32_t bmax[kMaxCols];      // B[m-1]
+  uint32_t shift[kMaxCols];     // bucket = (x - bmin) >> shift
+  uint32_t tab_off[kMaxCols];   // word offsets into the pass blob
+  uint32_t bnd_off[kMaxCols];
+  uint32_t bkt_off[kMaxCols];   // uint16 bucket starts, nbuckets+1 entries
+  int ncols;
+  uint32_t blob_words;          // words of the blob copied to shared memory
+  const uint32_t *blob;         // tables | boundaries | buckets | slot map (global)
+  uint32_t slot_off;            // word offset of the 256-entry slot -> query map
+  uint32_t *out;
+  uint64_t stride_words;
+  unsigned long long *counts;
+  uint64_t nrows;
+  uint64_t words;               // bitmap words of one query
+  uint64_t block_begin;         // first 256-row block of the range
+  uint64_t nblocks;             // end of the range, in 256-row blocks
+  int vec_store;                // bitmaps 16-byte aligned (out and stride)
+};
+
+// Position of x among the boundaries of column c: #{B[i] <= x}.
+__device__ __forceinline__ uint32_t position(const BatchPass &p, const uint32_t *sm, int c, uint32_t x) {
+  const uint32_t m = p.m[c];
+  if (m == 0 || x < p.bmin[c]) return 0;
+  if (x >= p.bmax[c]) return m;
+  const uint32_t k = (x - p.bmin[c]) >> p.shift[c];
+  const uint16_t *bk = reinterpret_cast<const uint16_t *>(sm + p.bkt_off[c]);
+  uint32_t lo = bk[k], hi = bk[k + 1];  // boundaries of bucket k: B[lo..hi)
+  const uint32_t *B = sm + p.bnd_off[c];
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (B[mid] <= x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// 8x8 bit transposes in each byte lane of eight registers: on return, bit r
+// of byte b of x[c] is bit c of byte b of the input x[r].
+__device__ __forceinline__ void transpose8x8x4(uint32_t (&x)[8]) {
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    uint32_t t = ((x[r] >> 4) ^ x[r + 4]) & 0x0F0F0F0Fu;
+    x[r + 4] ^= t;
+    x[r] ^= t << 4;
+  }
+#pragma unroll
+  for (int base = 0; base < 8; base += 4) {
+#pragma unroll
+    for (int r = base; r < base + 2; r++) {
+      uint32_t t = ((x[r] >> 2) ^ x[r + 2]) & 0x33333333u;
+      x[r + 2] ^= t;
+      x[r] ^= t << 2;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; r += 2) {
+    uint32_t t = ((x[r] >> 1) ^ x[r + 1]) & 0x55555555u;
+    x[r + 1] ^= t;
+    x[r] ^= t << 1;
+  }
+}
+
+// Staging layout per warp: slot q, tile t -> row = q/4 holds the 32 words of
+// slots 4*row..4*row+3 (8 tiles each) rotated by (row>>1)&31, so that both
+// the per-tile writes (32 lanes, 32 different slots) and the per-sector
+// reads (4 slots x 8 tiles) hit 32 different banks.
+__device__ __forceinline__ uint32_t stage_index(uint32_t slot, uint32_t t) {
+  const uint32_t row = slot >> 2;
+  const uint32_t col = ((slot & 3) * 8 + t + ((row >> 1) & 31)) & 31;
+  return row * 32 + col;
+}
+
+template <int CMAX>
+__global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ BatchPass p) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t *blob = smem;
+  uint32_t *stage_all = smem + ((p.blob_words + 3) & ~3u);
+  // positions of a warp's 32-row tile: row r at r*CMAX + (r/8)*CMAX words,
+  // so the four rows read together (s*8+i, s = 0..3) sit in different banks
+  uint32_t *posbuf_all = stage_all + kWarps * kStageWords;
+  unsigned int *cta_count = posbuf_all + kWarps * kPosWords<CMAX>;
+
+  for (uint32_t i = threadIdx.x; i < p.blob_words; i += blockDim.x) blob[i] = __ldg(p.blob + i);
+  for (int i = threadIdx.x; i < kSlots; i += blockDim.x) cta_count[i] = 0;
+  __syncthreads();
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = lane >> 3, g = lane & 7;
+  uint32_t *stage = stage_all + warp * kStageWords;
+  uint32_t *posbuf = posbuf_all + warp * kPosWords<CMAX>;
+  const int32_t *slot_query = reinterpret_cast<const int32_t *>(blob + p.slot_off);
+  const int C = p.ncols;
+  uint32_t tab_base[CMAX];  // this lane's word of table row 0, per column
+#pragma unroll
+  for (int c = 0; c < CMAX; c++) tab_base[c] = c < C ? p.tab_off[c] + g : 0u;
+  const bool vec_store = p.vec_store;
+  uint32_t cnt[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) cnt[k] = 0;
+
+  const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
+  const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+  for (uint64_t blk = p.block_begin + gwarp; blk < p.nblocks; blk += nwarps) {
+    const uint64_t row0 = blk * (32 * kTilesPerBlock);
+    // every column value of the block, loaded up front (lane = row in tile)
+    uint32_t v[kTilesPerBlock][CMAX];
+#pragma unroll
+    for (int t = 0; t < kTilesPerBlock; t++) {
+      const uint64_t row = row0 + 32 * t + lane;
+#pragma unroll
+      for (int c = 0; c < CMAX; c++)
+        v[t][c] = (c < C && row < p.nrows) ? __ldg(p.col[c] + row) : 0u;
+    }
+#pragma unroll
+    for (int t = 0; t < kTilesPerBlock; t++) {
+      const uint64_t tile_row0 = row0 + 32 * t;
+      // positions of this lane's row, one per column
+      {
+        uint32_t pv[CMAX];
+#pragma unroll
+        for (int c = 0; c < CMAX; c++) pv[c] = c < C ? position(p, blob, c, v[t][c]) : 0u;
+        uint32_t *dst = posbuf + lane * CMAX + (lane >> 3) * CMAX;
+#pragma unroll
+        for (int c = 0; c < CMAX; c += 4)
+          *reinterpret_cast<uint4 *>(dst + c) = make_uint4(pv[c], pv[c + 1], pv[c + 2], pv[c + 3]);
+      }
+      __syncwarp();
+      // masks of rows s*8+i for group g
+      uint32_t mk[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint32_t *pr = posbuf + (s * 8 + i) * CMAX + s * CMAX;
+        uint32_t pos[CMAX];
+#pragma unroll
+        for (int c = 0; c < CMAX; c += 4) {
+          const uint4 q4 = *reinterpret_cast<const uint4 *>(pr + c);
+          pos[c] = q4.x;
+          pos[c + 1] = q4.y;
+          pos[c + 2] = q4.z;
+          pos[c + 3] = q4.w;
+        }
+        uint32_t a = 0xFFFFFFFFu;
+#pragma unroll
+        for (int c = 0; c < CMAX; c++)
+          if (c < C) a &= blob[tab_base[c] + pos[c] * kGroups];
+        mk[7 - i] = a;  // reversed: bit r of the transposed byte is row 7-r
+      }
+      __syncwarp();
+      transpose8x8x4(mk);
+      // mk[c] byte b = 8 row bits (MSB = row s*8) of query 8b+c of group g.
+      // Lane s finalizes byte lane b = s: in round d it sends byte lane s^d
+      // of mk[0..3] and mk[4..7] (packed by byte permutes) to lane s^d of
+      // its group and receives byte lane s from that lane.  The bytes from
+      // round d belong at byte 3-d of V (static positions); the final word
+      // wants source lane s^d's rows at byte 3-(s^d), i.e. output byte p
+      // takes V's byte p^s.
+      uint32_t rlo[4], rhi[4];
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        const uint32_t dst = (uint32_t)(s ^ d);
+        const uint32_t sel = dst | ((dst + 4) << 4);
+        const uint32_t lo4 = __byte_perm(__byte_perm(mk[0], mk[1], sel), __byte_perm(mk[2], mk[3], sel), 0x5410);
+        const uint32_t hi4 = __byte_perm(__byte_perm(mk[4], mk[5], sel), __byte_perm(mk[6], mk[7], sel), 0x5410);
+        rlo[d] = d == 0 ? lo4 : __shfl_xor_sync(kFull, lo4, 8 * d);
+        rhi[d] = d == 0 ? hi4 : __shfl_xor_sync(kFull, hi4, 8 * d);
+      }
+      const uint32_t fix = (uint32_t)(0 ^ s) | ((uint32_t)(1 ^ s) << 4) | ((uint32_t)(2 ^ s) << 8) |
+                           ((uint32_t)(3 ^ s) << 12);
+      uint32_t w[8];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        // V byte 3-d = byte k of r[d]
+        const uint32_t selk = (uint32_t)k | ((uint32_t)(k + 4) << 4);
+        const uint32_t a = __byte_perm(rlo[3], rlo[2], selk);  // byte0 = r3.k, byte1 = r2.k
+        const uint32_t b = __byte_perm(rlo[1], rlo[0], selk);  // byte0 = r1.k, byte1 = r0.k
+        w[k] = __byte_perm(__byte_perm(a, b, 0x5410), 0, fix);
+        const uint32_t c2 = __byte_perm(rhi[3], rhi[2], selk);
+        const uint32_t d2 = __byte_perm(rhi[1], rhi[0], selk);
+        w[k + 4] = __byte_perm(__byte_perm(c2, d2, 0x5410), 0, fix);
+      }
+      // w[k] is the word of query slot 32g + 8s + k for rows tile_row0..+31
+      if (tile_row0 + 32 > p.nrows) {
+        const uint64_t valid = tile_row0 < p.nrows ? p.nrows - tile_row0 : 0;
+        const uint32_t vm = valid >= 32 ? 0xFFFFFFFFu : (valid ? ~(0xFFFFFFFFu >> valid) : 0u);
+#pragma unroll
+        for (int k = 0; k < 8; k++) w[k] &= vm;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        cnt[k] += __popc(w[k]);
+        stage[stage_index(32 * g + 8 * s + k, t)] = w[k];
+      }
+    }
+    __syncwarp();
+    // store: each lane writes one query's 8 words of this block (a full
+    // 32-byte sector) with two 16-byte stores when the bitmaps are aligned
+    const uint64_t word0 = blk * kTilesPerBlock;
+    const bool full = word0 + kTilesPerBlock <= p.words;
+#pragma unroll 2
+    for (int j = 0; j < kSlots / 32; j++) {
+      const uint32_t slot = 32 * j + lane;
+      const int32_t q = slot_query[slot];
+      uint32_t wv[kTilesPerBlock];
+#pragma unroll
+      for (int t = 0; t < kTilesPerBlock; t++) wv[t] = stage[stage_index(slot, t)];
+      if (q >= 0) {
+        uint32_t *dst = p.out + (uint64_t)q * p.stride_words + word0;
+        if (vec_store && full) {
+          reinterpret_cast<uint4 *>(dst)[0] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+          reinterpret_cast<uint4 *>(dst)[1] = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+        } else {
+#pragma unroll
+          for (int t = 0; t < kTilesPerBlock; t++)
+            if (word0 + t < p.words) dst[t] = wv[t];
+        }
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    if (cnt[k]) atomicAdd(&cta_count[32 * g + 8 * s + k], cnt[k]);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kSlots; i += blockDim.x) {
+    const int32_t q = slot_query[i];
+    if (q >= 0 && cta_count[i]) atomicAdd(p.counts + q, (unsigned long long)cta_count[i]);
+  }
+}
+
+template <int CMAX>
+size_t smem_bytes(uint32_t blob_words) {
+  return ((blob_words + 3) & ~3u) * 4 + (size_t)kWarps * kStageWords * 4 + (size_t)kWarps * kPosWords<CMAX> * 4 +
+         kSlots * 4;
+}
+
+template <int CMAX>
+int blocks_per_sm(size_t smem) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(batch_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr_set = true;
+  }
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<CMAX>, kThreads, smem) != cudaSuccess || b < 1)
+    b = 1;
+  return b;
+}
+
+// ---- host planning -----------------------------------------------------------
+
+struct NormQuery {
+  int index;                       // position in the caller's list
+  std::vector<int> cols;           // constrained columns
+  std::vector<uint32_t> lo, hi;
+  bool empty = false;
+};
+
+NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table) {
+  NormQuery q;
+  q.index = index;
+  std::vector<int> cols;
+  std::vector<uint32_t> lo, hi;
+  for (int i = 0; i < n; i++) {
+    const rts_term &t = terms[i];
+    if (t.column < 0 || t.column >= ncols_table) throw Error(RTS_ERR_ARG, "term column out of range");
+    if (t.lo > t.hi) q.empty = true;
+    auto it = std::find(cols.begin(), cols.end(), (int)t.column);
+    if (it == cols.end()) {
+      cols.push_back(t.column);
+      lo.push_back(t.lo);
+      hi.push_back(t.hi);
+    } else {
+      size_t k = it - cols.begin();
+      lo[k] = std::max(lo[k], t.lo);
+      hi[k] = std::min(hi[k], t.hi);
+      if (lo[k] > hi[k]) q.empty = true;
+    }
+  }
+  for (size_t k = 0; k < cols.size(); k++) {
+    if (lo[k] == 0 && hi[k] == 0xFFFFFFFFu) continue;
+    q.cols.push_back(cols[k]);
+    q.lo.push_back(lo[k]);
+    q.hi.push_back(hi[k]);
+  }
+  return q;
+}
+
+struct PassPlan {
+  std::vector<int> qs;                      // normalized queries (indices into the list)
+  std::vector<int> cols;                    // table columns, in order
+  std::vector<std::set<uint32_t>> bounds;   // per table column
+};
+
+// Shared-memory bytes of a pass's tables, boundaries and bucket index for
+// the given boundary counts (bucket index at most 4097 uint16 per column).
+size_t column_bytes(size_t m) {
+  size_t nb = 1;
+  while (nb < 4 * m && nb < 4096) nb <<= 1;
+  return (m + 1) * kGroups * 4 + m * 4 + (nb + 2) * 2 + 8;
+}
+
+// Add query q to the pass if its tables still fit the budget.
+bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget) {
+  if ((int)pp.qs.size() >= kSlots) return false;
+  size_t total = 0;
+  int new_cols = 0;
+  std::vector<size_t> grow(pp.cols.size(), 0);
+  std::vector<uint32_t> extra_new;  // boundaries of columns new to the pass
+  for (size_t k = 0; k < q.cols.size(); k++) {
+    auto it = std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]);
+    size_t add = 0;
+    if (it == pp.cols.end()) {
+      new_cols++;
+      add = (q.lo[k] > 0) + (q.hi[k] < 0xFFFFFFFFu);
+      total += column_bytes(add);
+    } else {
+      const auto &S = pp.bounds[it - pp.cols.begin()];
+      if (q.lo[k] > 0 && !S.count(q.lo[k])) grow[it - pp.cols.begin()]++;
+      if (q.hi[k] < 0xFFFFFFFFu && !S.count(q.hi[k] + 1)) grow[it - pp.cols.begin()]++;
+    }
+  }
+  if ((int)pp.cols.size() + new_cols > kMaxCols) return false;
+  for (size_t c = 0; c < pp.cols.size(); c++) total += column_bytes(pp.bounds[c].size() + grow[c]);
+  if (total > budget && !pp.qs.empty()) return false;
+  for (size_t k = 0; k < q.cols.size(); k++) {
+    auto it = std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]);
+    size_t ci;
+    if (it == pp.cols.end()) {
+      pp.cols.push_back(q.cols[k]);
+      pp.bounds.emplace_back();
+      ci = pp.cols.size() - 1;
+    } else {
+      ci = it - pp.cols.begin();
+    }
+    if (q.lo[k] > 0) pp.bounds[ci].insert(q.lo[k]);
+    if (q.hi[k] < 0xFFFFFFFFu) pp.bounds[ci].insert(q.hi[k] + 1);
+  }
+  pp.qs.push_back(qi);
+  return true;
+}
+
+}  // namespace
+
+// Device and pinned host buffers for batch plans, two of each so that the
+// plan of the next batch can be built and uploaded while the previous batch
+// still runs.
+struct BatchScratch {
+  struct Slot {
+    void *dev = nullptr;
+    size_t dev_cap = 0;
+    uint32_t *host = nullptr;
+    size_t host_cap = 0;
+    cudaEvent_t done = nullptr;
+  } slot[2];
+  int next = 0;
+  ~BatchScratch() {
+    for (auto &s : slot) {
+      if (s.done) cudaEventSynchronize(s.done);
+      if (s.dev) cudaFree(s.dev);
+      if (s.host) cudaFreeHost(s.host);
+      if (s.done) cudaEventDestroy(s.done);
+    }
+  }
+};
+
+void destroy_batch(BatchScratch *b) { delete b; }
+
+// A planned batch: the mask-table passes of the queries that run in the
+// kernel, built on the host once per query set.
+struct BatchPlan {
+  struct Pass {
+    BatchPass bp;
+    size_t off;  // word offset of the pass in `blob`
+    int cmax;
+  };
+  std::vector<Pass> passes;
+  std::vector<uint32_t> blob;
+};
+
+// Answer the queries that do not run in the batch kernel (empty, no
+// constrained column, more than eight constrained columns) over the whole
+// table; returns the kernels launched.
+int launch_outside(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
+                   const int32_t *out_index, uint32_t *out, uint64_t stride_words, unsigned long long *counts,
+                   cudaStream_t s) {
+  const uint64_t n = ctx->nrows;
+  int launches = 0;
+  for (int qi : which) {
+    const NormQuery &q = norm[qi];
+    const uint64_t o = out_index ? (uint64_t)out_index[qi] : (uint64_t)qi;
+    uint32_t *bm = out + o * stride_words;
+    if (q.empty || q.cols.empty()) {
+      launch_fill_range(bm, n, !q.empty, counts + o, ctx->sm_count, s);
+      launches += 2;
+      continue;
+    }
+    ScanParams sp;
+    memset(&sp, 0, sizeof sp);
+    for (size_t first = 0; first < q.cols.size(); first += kFusedMaxTerms) {
+      size_t cnt = std::min<size_t>(kFusedMaxTerms, q.cols.size() - first);
+      bool vec = true;
+      for (size_t i = 0; i < cnt; i++) {
+        sp.t[i] = {ctx->cols[q.cols[first + i]], q.lo[first + i], q.hi[first + i] - q.lo[first + i]};
+        vec = vec && (((uintptr_t)sp.t[i].col & 15) == 0);
+      }
+      sp.nterms = (int)cnt;
+      sp.and_into = first > 0;
+      sp.out = bm;
+      sp.count = first + cnt == q.cols.size() ? counts + o : nullptr;
+      sp.nrows = n;
+      sp.full_tiles = n / kTileRows;
+      if (first == 0) RTS_CUDA(cudaMemsetAsync(counts + o, 0, 8, s));
+      launch_scan_fused(sp, vec, ctx->sm_count, s);
+      launches++;
+    }
+  }
+  return launches;
+}
+
+bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && (int)q.cols.size() <= kMaxCols; }
+
+// Passes for the kernel queries `which` (indices into norm); query qi writes
+// bitmap out_index[qi] (qi when null).
+BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
+                     const int32_t *out_index, size_t table_budget) {
+  std::vector<PassPlan> passes;
+  for (int qi : which) {
+    if (passes.empty() || !try_add(passes.back(), norm[qi], qi, table_budget)) {
+      passes.emplace_back();
+      if (!try_add(passes.back(), norm[qi], qi, table_budget))
+        throw Error(RTS_ERR_ARG, "query does not fit one batch pass");
+    }
+  }
+  BatchPlan plan;
+  for (auto &pp : passes) {
+    BatchPlan::Pass b;
+    memset(&b.bp, 0, sizeof b.bp);
+    BatchPass &bp = b.bp;
+    const int C = (int)pp.cols.size();
+    bp.ncols = C;
+    std::vector<uint32_t> blob;
+    std::vector<std::vector<uint32_t>> B(C);
+    for (int c = 0; c < C; c++) B[c].assign(pp.bounds[c].begin(), pp.bounds[c].end());
+    // tables: row pos holds, per slot, whether the values of interval pos
+    // ([B[pos-1], B[pos]) with B[-1] = 0, B[m] = 2^32) pass the slot's term
+    // on this column (always, when the slot does not constrain it).  Built
+    // as XOR deltas at the interval ends and a prefix XOR over positions.
+    for (int c = 0; c < C; c++) {
+      const uint32_t m = (uint32_t)B[c].size();
+      bp.m[c] = m;
+      bp.tab_off[c] = (uint32_t)blob.size();
+      blob.resize(blob.size() + (size_t)(m + 1) * kGroups, 0u);
+      std::vector<uint32_t> delta((size_t)(m + 2) * kGroups, 0u);
+      auto pos_of = [&](uint32_t x) {  // #boundaries <= x
+        return (uint32_t)(std::upper_bound(B[c].begin(), B[c].end(), x) - B[c].begin());
+      };
+      for (int slot = 0; slot < (int)pp.qs.size(); slot++) {
+        const NormQuery &q = norm[pp.qs[slot]];
+        auto it = std::find(q.cols.begin(), q.cols.end(), pp.cols[c]);
+        const uint32_t bit = 1u << (slot & 31);
+        const int grp = slot >> 5;
+        uint32_t p0 = 0, p1 = m;  // positions covered, inclusive
+        if (it != q.cols.end()) {
+          const size_t k = it - q.cols.begin();
+          p0 = pos_of(q.lo[k]);
+          p1 = pos_of(q.hi[k]);
+        }
+        delta[(size_t)p0 * kGroups + grp] ^= bit;
+        delta[(size_t)(p1 + 1) * kGroups + grp] ^= bit;
+      }
+      uint32_t *tab = blob.data() + bp.tab_off[c];
+      for (int grp = 0; grp < kGroups; grp++) {
+        uint32_t acc = 0;
+        for (uint32_t pos = 0; pos <= m; pos++) {
+          acc ^= delta[(size_t)pos * kGroups + grp];
+          tab[(size_t)pos * kGroups + grp] = acc;
+        }
+      }
+    }
+    // boundaries and bucket index
+    for (int c = 0; c < C; c++) {
+      const uint32_t m = bp.m[c];
+      bp.bnd_off[c] = (uint32_t)blob.size();
+      blob.insert(blob.end(), B[c].begin(), B[c].end());
+      if (m == 0) {
+        bp.bkt_off[c] = (uint32_t)blob.size();
+        blob.push_back(0);
+        continue;
+      }
+      bp.bmin[c] = B[c].front();
+      bp.bmax[c] = B[c].back();
+      const uint64_t span = (uint64_t)bp.bmax[c] - bp.bmin[c] + 1;
+      uint32_t nb_target = 1;
+      while (nb_target < 4 * m && nb_target < 4096) nb_target <<= 1;
+      uint32_t shift = 0;
+      while ((span >> shift) > nb_target) shift++;
+      bp.shift[c] = shift;
+      const uint32_t nb = (uint32_t)(((span - 1) >> shift) + 1);  // buckets covering [bmin, bmax]
+      std::vector<uint16_t> bk(nb + 1);
+      for (uint32_t k = 0; k <= nb; k++) {
+        const uint64_t start = (uint64_t)bp.bmin[c] + ((uint64_t)k << shift);
+        bk[k] = (uint16_t)(std::lower_bound(B[c].begin(), B[c].end(), start) - B[c].begin());
+        if (start > 0xFFFFFFFFull) bk[k] = (uint16_t)m;
+      }
+      bp.bkt_off[c] = (uint32_t)blob.size();
+      const size_t wsz = (bk.size() + 1) / 2;
+      blob.resize(blob.size() + wsz, 0u);
+      memcpy(blob.data() + bp.bkt_off[c], bk.data(), bk.size() * 2);
+    }
+    bp.slot_off = (uint32_t)blob.size();
+    for (int slot = 0; slot < kSlots; slot++) {
+      uint32_t o = 0xFFFFFFFFu;
+      if (slot < (int)pp.qs.size()) o = out_index ? (uint32_t)out_index[pp.qs[slot]] : (uint32_t)pp.qs[slot];
+      blob.push_back(o);
+    }
+    bp.blob_words = (uint32_t)blob.size();
+    for (int c = 0; c < C; c++) bp.col[c] = ctx->cols[pp.cols[c]];
+    b.cmax = C <= 4 ? 4 : 8;
+    while (plan.blob.size() % 4) plan.blob.push_back(0);  // 16-byte aligned pass start
+    b.off = plan.blob.size();
+    plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
+    plan.passes.push_back(b);
+  }
+  return plan;
+}
+
+// Launch every pass of `plan` (blob already on the device) over rows
+// [row_begin, row_end); row_begin is a multiple of 256.  Returns launches.
+int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
+                unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
+  const uint64_t rows_per_block = 32 * kTilesPerBlock;
+  int launches = 0;
+  for (auto &b : plan.passes) {
+    BatchPass bp = b.bp;
+    bp.blob = dev_blob + b.off;
+    bp.out = out;
+    bp.stride_words = stride_words;
+    bp.counts = counts;
+    bp.nrows = row_end;
+    bp.words = words_for(ctx->nrows);
+    bp.block_begin = row_begin / rows_per_block;
+    bp.nblocks = (row_end + rows_per_block - 1) / rows_per_block;
+    bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
+    const uint64_t want = (bp.nblocks - bp.block_begin + kWarps - 1) / kWarps;
+    if (b.cmax == 4) {
+      const size_t sm = smem_bytes<4>(bp.blob_words);
+      const int per = blocks_per_sm<4>(sm);
+      const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per * ctx->sm_count));
+      batch_kernel<4><<<grid, kThreads, sm, s>>>(bp);
+    } else {
+      const size_t sm = smem_bytes<8>(bp.blob_words);
+      const int per = blocks_per_sm<8>(sm);
+      const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per * ctx->sm_count));
+      batch_kernel<8><<<grid, kThreads, sm, s>>>(bp);
+    }
+    launches++;
+  }
+  return launches;
+}
+
+std::vector<NormQuery> normalize_all(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq) {
+  std::vector<NormQuery> norm;
+  norm.reserve(nq);
+  for (int q = 0; q < nq; q++) {
+    if (offsets[q + 1] < offsets[q] || offsets[q] < 0) throw Error(RTS_ERR_ARG, "offsets not ascending");
+    norm.push_back(normalize(terms + offsets[q], offsets[q + 1] - offsets[q], q, (int)ctx->cols.size()));
+  }
+  return norm;
+}
+
+// Copy `plan` to one of the context's two plan buffers (pinned staging +
+// device), waiting for the batch that used that buffer two calls ago.
+const uint32_t *upload_plan(rts_ctx *ctx, const BatchPlan &plan, cudaStream_t s, cudaEvent_t *done) {
+  if (!ctx->batch) ctx->batch = new BatchScratch();
+  BatchScratch::Slot &S = ctx->batch->slot[ctx->batch->next];
+  ctx->batch->next ^= 1;
+  const size_t bytes = std::max<size_t>(plan.blob.size(), 4) * 4;
+  if (S.done) RTS_CUDA(cudaEventSynchronize(S.done));
+  else RTS_CUDA(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+  if (S.dev_cap < bytes) {
+    if (S.dev) cudaFree(S.dev);
+    S.dev = nullptr;
+    S.dev_cap = 0;
+    if (cudaMalloc(&S.dev, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(RTS_ERR_NOMEM, "batch plan allocation failed");
+    }
+    S.dev_cap = bytes;
+  }
+  if (S.host_cap < bytes) {
+    if (S.host) cudaFreeHost(S.host);
+    S.host = nullptr;
+    S.host_cap = 0;
+    RTS_CUDA(cudaMallocHost(&S.host, bytes));
+    S.host_cap = bytes;
+  }
+  memcpy(S.host, plan.blob.data(), plan.blob.size() * 4);
+  RTS_CUDA(cudaMemcpyAsync(S.dev, S.host, plan.blob.size() * 4, cudaMemcpyHostToDevice, s));
+  *done = S.done;
+  return reinterpret_cast<const uint32_t *>(S.dev);
+}
+
+void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq, uint32_t *out,
+                uint64_t stride_words, unsigned long long *counts, cudaStream_t s, size_t table_budget) {
+  std::vector<NormQuery> norm = normalize_all(ctx, terms, offsets, nq);
+  std::vector<int> inside, outside;
+  for (int q = 0; q < nq; q++) (runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
+  int launches = launch_outside(ctx, norm, outside, nullptr, out, stride_words, counts, s);
+  if (!inside.empty()) {
+    RTS_CUDA(cudaMemsetAsync(counts, 0, (size_t)nq * 8, s));
+    BatchPlan plan = build_plan(ctx, norm, inside, nullptr, table_budget);
+    cudaEvent_t done = nullptr;
+    const uint32_t *dev_blob = upload_plan(ctx, plan, s, &done);
+    launches += launch_plan(ctx, plan, dev_blob, out, stride_words, counts, 0, ctx->nrows, s);
+    RTS_CUDA(cudaEventRecord(done, s));
+  }
+  RTS_CUDA(cudaGetLastError());
+  ctx->launches += launches;
+}
+
+}  // namespace rts
+
+namespace rts {
+// Device buffers of the host-buffer batch call, kept by the context.
+struct HostBatchBuffers {
+  uint32_t *cols = nullptr;
+  size_t cols_cap = 0;
+  uint32_t *bitmaps = nullptr;
+  size_t bm_cap = 0;
+  unsigned long long *counts = nullptr;
+  size_t cnt_cap = 0;
+  cudaStream_t compute = nullptr, copy = nullptr;
+  std::vector<cudaEvent_t> ev;
+  ~HostBatchBuffers() {
+    if (cols) cudaFree(cols);
+    if (bitmaps) cudaFree(bitmaps);
+    if (counts) cudaFree(counts);
+    for (auto e : ev) cudaEventDestroy(e);
+    if (compute) cudaStreamDestroy(compute);
+    if (copy) cudaStreamDestroy(copy);
+  }
+};
+void destroy_host_batch(HostBatchBuffers *b) { delete b; }
+
+template <class T>
+static void ensure(T *&p, size_t &cap, size_t count) {
+  if (cap >= count) return;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(RTS_ERR_NOMEM, "device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
+  }
+  cap = count;
+}
+}  // namespace rts
+
+// Host columns in, host bitmaps out: upload, batched passes, download, with
+// the download of each chunk of queries overlapping the next chunk's pass.
+extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
+                                          uint64_t nrows, const rts_term *terms, const int32_t *offsets, int32_t nq,
+                                          uint32_t *host_bitmaps, uint64_t stride_words, uint64_t *host_counts) {
+  if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
+  try {
+    if (!host_cols || ncols < 1 || nrows == 0) throw rts::Error(RTS_ERR_ARG, "need host columns");
+    for (int c = 0; c < ncols; c++)
+      if (!host_cols[c]) throw rts::Error(RTS_ERR_ARG, "null column pointer");
+    if (nq < 0 || (nq > 0 && (!offsets || !host_bitmaps || !host_counts)))
+      throw rts::Error(RTS_ERR_ARG, "bad batch arguments");
+    const uint64_t words = rts::words_for(nrows);
+    if (stride_words < words) throw rts::Error(RTS_ERR_ARG, "stride_words smaller than a bitmap");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    if (!ctx->host_batch) ctx->host_batch = new rts::HostBatchBuffers();
+    rts::HostBatchBuffers &H = *ctx->host_batch;
+    if (!H.compute) RTS_CUDA(cudaStreamCreateWithFlags(&H.compute, cudaStreamNonBlocking));
+    if (!H.copy) RTS_CUDA(cudaStreamCreateWithFlags(&H.copy, cudaStreamNonBlocking));
+    const uint64_t cstride = (nrows + 3) / 4 * 4;
+    rts::ensure(H.cols, H.cols_cap, (size_t)cstride * ncols);
+    rts::ensure(H.bitmaps, H.bm_cap, (size_t)std::max(nq, 1) * stride_words);
+    rts::ensure(H.counts, H.cnt_cap, (size_t)std::max(nq, 1));
+    for (int c = 0; c < ncols; c++)
+      RTS_CUDA(cudaMemcpyAsync(H.cols + cstride * c, host_cols[c], nrows * 4, cudaMemcpyHostToDevice, H.compute));
+    // The batch kernels read the uploaded columns through the context.
+    std::vector<const uint32_t *> saved_cols = ctx->cols;
+    const uint64_t saved_n = ctx->nrows;
+    ctx->cols.clear();
+    for (int c = 0; c < ncols; c++) ctx->cols.push_back(H.cols + cstride * c);
+    ctx->nrows = nrows;
+    struct Restore {
+      rts_ctx *c;
+      std::vector<const uint32_t *> cols;
+      uint64_t n;
+      ~Restore() {
+        c->cols = cols;
+        c->nrows = n;
+      }
+    } restore{ctx, saved_cols, saved_n};
+    const int chunk = 256;
+    const int nchunks = (nq + chunk - 1) / chunk;
+    while ((int)H.ev.size() < nchunks) {
+      cudaEvent_t e;
+      RTS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      H.ev.push_back(e);
+    }
+    for (int k = 0; k < nchunks; k++) {
+      const int q0 = k * chunk, q1 = std::min(nq, q0 + chunk);
+      std::vector<int32_t> off(offsets + q0, offsets + q1 + 1);
+      for (auto &o : off) o -= offsets[q0];
+      rts::batch_scan(ctx, terms + offsets[q0], off.data(), q1 - q0, H.bitmaps + (uint64_t)q0 * stride_words,
+                      stride_words, H.counts + q0, H.compute, ctx->batch_table_budget);
+      RTS_CUDA(cudaEventRecord(H.ev[k], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[k], 0));
+      RTS_CUDA(cudaMemcpyAsync(host_bitmaps + (uint64_t)q0 * stride_words, H.bitmaps + (uint64_t)q0 * stride_words,
+                               (uint64_t)(q1 - q0) * stride_words * 4, cudaMemcpyDeviceToHost, H.copy));
+    }
+    if (nq > 0)
+      RTS_CUDA(cudaMemcpyAsync(host_counts, H.counts, (size_t)nq * 8, cudaMemcpyDeviceToHost, H.copy));
+    RTS_CUDA(cudaStreamSynchronize(H.copy));
+    RTS_CUDA(cudaStreamSynchronize(H.compute));
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return RTS_OK;
+  } catch (const rts::Error &e) {
+    ctx->err = e.what();
+    return rts::set_thread_error(e.code, e.what());
+  } catch (const std::exception &e) {
+    ctx->err = e.what();
+    return rts::set_thread_error(RTS_ERR_NOMEM, e.what());
+  }
+}
+
+extern "C" rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
+                                           uint32_t *dev_bitmaps, uint64_t stride_words, uint64_t *dev_counts,
+                                           void *stream) {
+  if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
+  try {
+    if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");
+    if (nq < 0 || (nq > 0 && (!offsets || !dev_bitmaps || !dev_counts)))
+      throw rts::Error(RTS_ERR_ARG, "bad batch arguments");
+    if (stride_words < rts::words_for(ctx->nrows)) throw rts::Error(RTS_ERR_ARG, "stride_words smaller than a bitmap");
+    if (nq == 0) return RTS_OK;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::batch_scan(ctx, terms, offsets, nq, dev_bitmaps, stride_words,
+                    reinterpret_cast<unsigned long long *>(dev_counts), (cudaStream_t)stream, ctx->batch_table_budget);
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    return RTS_OK;
+  } catch (const rts::Error &e) {
+    ctx->err = e.what();
+    return rts::set_thread_error(e.code, e.what());
+  } catch (const std::exception &e) {
+    ctx->err = e.what();
+    return rts::set_thread_error(RTS_ERR_NOMEM, e.what());
+  }
+}

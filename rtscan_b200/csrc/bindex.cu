@@ -719,10 +719,5 @@ rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nt
   }
 }
 
-rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *, const int32_t *, int32_t, uint32_t *, uint64_t,
-                                uint64_t *, void *) {
-  if (ctx) ctx->err = "batched scan is not available in this build";
-  return RTS_ERR_STATE;
-}
 
 }  // extern "C"

@@ -95,6 +95,17 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
 // A 256-byte device buffer owned by the context (blocking-call counts).
 unsigned long long *small_device_buffer(rts_ctx *ctx);
 
+// ---- batched scan (batch.cu) ----
+struct BatchScratch;
+void destroy_batch(BatchScratch *b);
+struct HostBatchBuffers;
+void destroy_host_batch(HostBatchBuffers *b);
+// Shared-memory bytes one batch pass may spend on its mask tables; the
+// rest of the CTA's shared memory stages result words.
+constexpr size_t kDefaultBatchTableBudget = 88 * 1024;
+void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq, uint32_t *out,
+                uint64_t stride_words, unsigned long long *counts, cudaStream_t s, size_t table_budget);
+
 }  // namespace rts
 
 // The context.  Defined here so every translation unit sees one layout.
@@ -114,6 +125,9 @@ struct rts_ctx {
   size_t plan_bytes = 0;
   void *plan_host = nullptr;  // pinned
   void *small_dev = nullptr;
+  rts::BatchScratch *batch = nullptr;
+  rts::HostBatchBuffers *host_batch = nullptr;
+  size_t batch_table_budget = rts::kDefaultBatchTableBudget;
   std::atomic<uint64_t> launches{0};
   std::string err;
   ~rts_ctx();

@@ -1,0 +1,129 @@
+"""Batched scan (one pass answering many queries) against the oracle: every
+query's bitmap and count must equal the scalar filter's, whatever the batch
+size, the mix of column counts, or the pass split."""
+import numpy as np
+import pytest
+
+import rtscan_b200 as R
+from oracle import oracle as O
+from rtscan_b200 import datagen as D
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def expect(cols, terms):
+    n = len(cols[0])
+    if any(lo > hi for _, lo, hi in terms):
+        return np.zeros(O.words(n), np.uint32), 0
+    if not terms:
+        return O.mask_tail(np.full(O.words(n), 0xFFFFFFFF, np.uint32), n), n
+    return O.range_scan([cols[c] for c, _, _ in terms], [t[1] for t in terms], [t[2] for t in terms])
+
+
+def run_batch(ctx, queries, fn="batch"):
+    n = ctx.nrows
+    words = R.bitmap_words(n)
+    stride = words + 5  # deliberately not a multiple of anything
+    out = torch.full((max(1, len(queries)) * stride,), -1, dtype=torch.int32, device="cuda")
+    cnt = torch.full((max(1, len(queries)),), -1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    runner = ctx.scan_batch_async if fn == "batch" else ctx.scan_each_async
+    runner(queries, out.data_ptr(), stride, cnt.data_ptr(), s)
+    torch.cuda.synchronize()
+    o = out.cpu().numpy().view(np.uint32)
+    return [(o[i * stride:i * stride + words], int(cnt[i].item()), o[i * stride + words:(i + 1) * stride])
+            for i in range(len(queries))]
+
+
+def check_batch(ctx, cols, queries):
+    res = run_batch(ctx, queries)
+    for i, q in enumerate(queries):
+        want, wcnt = expect(cols, q)
+        got, cnt, pad = res[i]
+        assert cnt == wcnt, (i, q, cnt, wcnt)
+        assert np.array_equal(got, want), (i, q)
+        assert (pad == 0xFFFFFFFF).all(), "wrote past the bitmap"
+
+
+@pytest.mark.parametrize("nq", [1, 5, 31, 32, 33, 255, 256, 257, 700])
+def test_batch_sizes(ctx, nq):
+    n = 300_000 + 123
+    cols = [D.uniform(n, 1), D.zipf(n, 2, 1.3), D.uniform(n, 3, 256), D.normal(n, 4)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, nq, seed=nq)
+    check_batch(ctx, cols, qs)
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 255, 256, 257, 1000, 8191, 65537])
+def test_batch_row_counts(ctx, n):
+    cols = [D.uniform(n, 10 + n), D.uniform(n, 20 + n, 64)]
+    ctx.load_columns(cols)
+    s0 = np.sort(cols[0])
+    qs = [[(0, int(s0[0]), int(s0[-1]))], [(1, 3, 40)], [(0, 0, 1 << 31), (1, 10, 63)], [(1, 0, 0)],
+          [(0, int(s0[len(s0) // 2]), 0xFFFFFFFF)]]
+    check_batch(ctx, cols, qs)
+
+
+def test_batch_special_queries(ctx):
+    n = 100_003
+    cols = [D.uniform(n, c + 50, [1 << 32, 256, 64, 1 << 20, 7, 1 << 32, 1000, 1 << 16, 300, 99][c]) for c in range(10)]
+    ctx.load_columns(cols)
+    qs = [
+        [],                                        # no terms: all rows
+        [(0, 0, 0xFFFFFFFF)],                      # always true
+        [(1, 10, 5)],                              # empty term
+        [(0, 5, 10), (0, 20, 30)],                 # disjoint ranges on one column: empty
+        [(1, 10, 200), (1, 100, 255)],             # overlapping ranges merged
+        [(c, 1, [1 << 31, 200, 60, 1 << 19, 6, 1 << 31, 900, 1 << 15, 250, 90][c]) for c in range(10)],  # 10 columns
+        [(c, 0, [1 << 31, 200, 60, 1 << 19, 6, 1 << 31, 900, 1 << 15, 250, 90][c]) for c in range(9)],
+        [(4, 3, 3)],
+        [(2, 63, 63), (3, 0, 0)],
+    ] + D.batch_queries(cols[:4], 40, seed=9)
+    check_batch(ctx, cols, qs)
+
+
+def test_batch_many_columns_per_pass(ctx):
+    """Queries over 6 different columns force passes with more than 4 table columns."""
+    n = 50_000
+    cols = [D.uniform(n, 70 + c, 1 << (8 + 4 * c)) for c in range(6)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 300, seed=11, min_cols=1, max_cols=6)
+    check_batch(ctx, cols, qs)
+
+
+def test_batch_duplicate_heavy(ctx):
+    n = 200_000
+    cols = [D.uniform(n, 80, 2), D.uniform(n, 81, 64), D.zipf(n, 82, 1.5)]
+    ctx.load_columns(cols)
+    qs = []
+    for a in range(0, 64, 3):
+        qs.append([(1, a, a)])
+        qs.append([(1, a, 63), (0, 1, 1)])
+        qs.append([(2, a, a + 5), (0, 0, 0)])
+    check_batch(ctx, cols, qs)
+
+
+def test_batch_equals_each(ctx):
+    n = 1 << 20
+    cols = [D.zipf(n, 90, 1.1), D.zipf(n, 91, 1.3), D.zipf(n, 92, 1.5), D.normal(n, 93)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 1024, seed=3)
+    a = run_batch(ctx, qs, "batch")
+    b = run_batch(ctx, qs, "each")
+    for i in range(len(qs)):
+        assert a[i][1] == b[i][1], i
+        assert np.array_equal(a[i][0], b[i][0]), i
+
+
+def test_batch_alone_and_in_the_mix(ctx):
+    """A query's result does not depend on the other queries of its batch."""
+    n = 400_000
+    cols = [D.uniform(n, 95), D.normal(n, 96)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 600, seed=12)
+    mixed = run_batch(ctx, qs)
+    for i in (0, 17, 255, 256, 599):
+        alone = run_batch(ctx, [qs[i]])[0]
+        assert alone[1] == mixed[i][1]
+        assert np.array_equal(alone[0], mixed[i][0])
