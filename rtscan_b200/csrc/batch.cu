@@ -33,6 +33,7 @@
 #include <set>
 #include <vector>
 
+#include "batch_plan.h"
 #include "rts_internal.h"
 
 namespace rts {
@@ -300,14 +301,9 @@ int blocks_per_sm(size_t smem) {
   return b;
 }
 
-// ---- host planning -----------------------------------------------------------
+}  // namespace
 
-struct NormQuery {
-  int index;                       // position in the caller's list
-  std::vector<int> cols;           // constrained columns
-  std::vector<uint32_t> lo, hi;
-  bool empty = false;
-};
+// ---- host planning -----------------------------------------------------------
 
 NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table) {
   NormQuery q;
@@ -338,6 +334,8 @@ NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table) {
   }
   return q;
 }
+
+namespace {
 
 struct PassPlan {
   std::vector<int> qs;                      // normalized queries (indices into the list)
@@ -659,9 +657,10 @@ void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int
   std::vector<NormQuery> norm = normalize_all(ctx, terms, offsets, nq);
   std::vector<int> inside, outside;
   for (int q = 0; q < nq; q++) (runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
+  // every count starts at zero; the kernel accumulates, fills overwrite
+  RTS_CUDA(cudaMemsetAsync(counts, 0, (size_t)nq * 8, s));
   int launches = launch_outside(ctx, norm, outside, nullptr, out, stride_words, counts, s);
   if (!inside.empty()) {
-    RTS_CUDA(cudaMemsetAsync(counts, 0, (size_t)nq * 8, s));
     BatchPlan plan = build_plan(ctx, norm, inside, nullptr, table_budget);
     cudaEvent_t done = nullptr;
     const uint32_t *dev_blob = upload_plan(ctx, plan, s, &done);
@@ -670,6 +669,20 @@ void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int
   }
   RTS_CUDA(cudaGetLastError());
   ctx->launches += launches;
+}
+
+void BatchPlanDeleter::operator()(BatchPlan *p) const { delete p; }
+
+BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
+                             const int32_t *out_index, size_t table_budget) {
+  return BatchPlanPtr(new BatchPlan(build_plan(ctx, norm, which, out_index, table_budget)));
+}
+
+const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan) { return plan.blob; }
+
+int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
+                      unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
+  return launch_plan(ctx, plan, dev_blob, out, stride_words, counts, row_begin, row_end, s);
 }
 
 }  // namespace rts

@@ -1,0 +1,50 @@
+// Host-side planning interface of the batched kernel (batch.cu), shared
+// with the serving loop (serve.cpp).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "rts_internal.h"
+
+namespace rts {
+
+// A query after validation: terms merged per column (ranges intersected),
+// always-true terms dropped.
+struct NormQuery {
+  int index = 0;                   // position in the caller's list
+  std::vector<int> cols;           // constrained columns
+  std::vector<uint32_t> lo, hi;
+  bool empty = false;              // some term can never match
+};
+
+NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table);
+std::vector<NormQuery> normalize_all(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq);
+// True when the batched kernel answers the query (non-empty, 1..8 columns);
+// the others go through launch_outside.
+bool runs_in_kernel(const NormQuery &q);
+
+// Answer queries `which` (indices into norm) over the whole table with fill
+// or fused-scan launches; query qi writes bitmap / count out_index[qi] (qi
+// when out_index is null).  Returns the kernels launched.
+int launch_outside(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
+                   const int32_t *out_index, uint32_t *out, uint64_t stride_words, unsigned long long *counts,
+                   cudaStream_t s);
+
+// Mask-table passes for the kernel queries `which`, built on the host.
+struct BatchPlan;
+struct BatchPlanDeleter {
+  void operator()(BatchPlan *p) const;
+};
+using BatchPlanPtr = std::unique_ptr<BatchPlan, BatchPlanDeleter>;
+BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
+                             const int32_t *out_index, size_t table_budget);
+// The words to upload to the device before launching.
+const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan);
+// Launch every pass over rows [row_begin, row_end) (row_begin a multiple of
+// 256) with the plan blob at dev_blob; counts are accumulated (not reset).
+int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out,
+                      uint64_t stride_words, unsigned long long *counts, uint64_t row_begin, uint64_t row_end,
+                      cudaStream_t s);
+
+}  // namespace rts
