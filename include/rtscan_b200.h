@@ -235,6 +235,31 @@ RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, cons
                                        int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
                                        uint64_t *dev_counts, void *stream);
 
+/* ---- allocation-free scan ------------------------------------------------ */
+
+/* Largest row count rts_scan_separate_noalloc_async accepts (2^27 rows; its
+ * scratch bitmap is a fixed 16 MiB device array). */
+#define RTS_NOALLOC_MAX_ROWS (1ull << 27)
+/* No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory -- an engine that hands all of HBM to its own pool
+ * allocator at start-up, or a latency-critical caller that cannot afford
+ * cudaMalloc's device-wide synchronisation -- this computes the result of
+ * rts_scan_separate_async without a context and without allocating: plain
+ * device column pointers in (`ncols` columns of `nrows` values on the
+ * current device), caller-owned dev_bitmap (rts_bitmap_words(nrows) words)
+ * and *dev_count out, asynchronously on `stream`.  Its scratch bitmap is a
+ * file-scope __device__ array of RTS_NOALLOC_MAX_ROWS/8 bytes that every GPU
+ * loading this library holds until the process exits; nrows above
+ * RTS_NOALLOC_MAX_ROWS is rejected with RTS_ERR_ARG.  The first call on a
+ * device looks up that array's device address (once per device, with the
+ * device current), so make it before capturing any stream.  Every call
+ * shares the one array and the array keeps the last call's contents: the
+ * scan overwrites the words it reads, but calls that overlap on the GPU
+ * (different streams, or several host threads) race on it. */
+RTS_API rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev_cols, int32_t ncols,
+                                                   uint64_t nrows, const rts_term *terms, int32_t nterms,
+                                                   uint32_t *dev_bitmap, uint64_t *dev_count, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,8 @@ _SIGS = [
     ("rts_scan_batch_host", ctypes.c_int32, [_P, ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64, _TERMP,
                                              ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P, ctypes.c_uint64,
                                              _P]),
+    ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
+                                                         _TERMP, ctypes.c_int32, _P, _P, _P]),
 ]
 
 
