@@ -235,6 +235,49 @@ RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, cons
                                        int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
                                        uint64_t *dev_counts, void *stream);
 
+/* ---- serving: continuous batching over resident columns ----------------- */
+/* No reference counterpart (the reference drivers answer one query at a time,
+ * bindex_cuda.cpp:1827-1986).  A server owns a worker thread that runs the
+ * batched kernel as a circular scan over segments of the context's table:
+ * requests are admitted into result slots as slots free up, join the scan
+ * at the next segment, and are done when the scan has covered every
+ * segment once for them.  While a server runs, its context must not be used
+ * for other calls. */
+typedef struct rts_server_config {
+  int32_t max_active;         /* result slots (bitmap + count each); default 512 */
+  int32_t max_queue;          /* requests waiting for a slot before RTS_ERR_FULL; default 65536 */
+  uint64_t segment_rows;      /* rows per scan step, a multiple of 256; default 2^22 */
+  int32_t max_inflight_steps; /* steps queued on the GPU at once; default 2 */
+} rts_server_config;
+
+typedef struct rts_server_stats {
+  uint64_t submitted, completed, rejected, cancelled, steps, queued;
+  uint32_t active;
+  double p50_ms, p99_ms, p999_ms, max_ms, mean_ms; /* submit-to-done latency of completed requests */
+} rts_server_stats;
+
+/* cfg may be NULL (defaults); zero fields take their defaults. */
+RTS_API rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_server **out);
+/* Queue one conjunctive query; safe from many threads.  RTS_ERR_FULL when the
+ * queue holds max_queue requests. */
+RTS_API rts_status rts_server_submit(rts_server *srv, const rts_term *terms, int32_t nterms, uint64_t *ticket);
+RTS_API rts_status rts_server_poll(rts_server *srv, uint64_t ticket, int32_t *done, uint64_t *count);
+/* Block until the request is done (RTS_ERR_TIMEOUT after timeout_ms). */
+RTS_API rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms, uint64_t *count);
+/* Copy a done request's bitmap (rts_bitmap_words(nrows) words; NULL to skip)
+ * and count to the host and release its slot. */
+RTS_API rts_status rts_server_fetch(rts_server *srv, uint64_t ticket, uint32_t *host_bitmap, uint64_t *count);
+RTS_API rts_status rts_server_cancel(rts_server *srv, uint64_t ticket);
+RTS_API rts_status rts_server_get_stats(rts_server *srv, rts_server_stats *stats);
+/* Stop the worker and free the server (pending requests are dropped). */
+RTS_API rts_status rts_server_stop(rts_server *srv);
+/* Open-loop load replay for benchmarks: query q (CSR terms) is submitted
+ * arrival_s[q] seconds after the call starts and released as soon as it is
+ * done; latency_ms[q] gets its submit-to-done time (-1 if the queue was
+ * full).  Blocks until all are done. */
+RTS_API rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets,
+                                     int32_t nqueries, const double *arrival_s, double *latency_ms);
+
 /* ---- allocation-free scan ------------------------------------------------ */
 
 /* Largest row count rts_scan_separate_noalloc_async accepts (2^27 rows; its

@@ -43,6 +43,22 @@ class Term(ctypes.Structure):
         return f"Term(col={self.column}, lo={self.lo}, hi={self.hi})"
 
 
+class ServerConfig(ctypes.Structure):
+    """rts_server_config (zero fields take the library defaults)."""
+    _fields_ = [("max_active", ctypes.c_int32), ("max_queue", ctypes.c_int32), ("segment_rows", ctypes.c_uint64),
+                ("max_inflight_steps", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("cancelled", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("queued", ctypes.c_uint64),
+                ("active", ctypes.c_uint32), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("p999_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = ctypes.c_void_p
 _U32P = ctypes.POINTER(ctypes.c_uint32)
 _U64P = ctypes.POINTER(ctypes.c_uint64)
@@ -93,6 +109,16 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_server_start", ctypes.c_int32, [_P, ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    ("rts_server_submit", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, _U64P]),
+    ("rts_server_poll", ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), _U64P]),
+    ("rts_server_wait", ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.c_int32, _U64P]),
+    ("rts_server_fetch", ctypes.c_int32, [_P, ctypes.c_uint64, _P, _U64P]),
+    ("rts_server_cancel", ctypes.c_int32, [_P, ctypes.c_uint64]),
+    ("rts_server_get_stats", ctypes.c_int32, [_P, ctypes.POINTER(ServerStats)]),
+    ("rts_server_stop", ctypes.c_int32, [_P]),
+    ("rts_server_replay", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 ]
 
 
@@ -210,6 +236,83 @@ class PreparedQueries:
 
 def prepare(queries) -> PreparedQueries:
     return PreparedQueries(queries)
+
+
+class Server:
+    """Continuous-batching scan server over a context's resident columns
+    (rts_server_*).  The context must not be used for other calls while the
+    server runs."""
+
+    def __init__(self, ctx: "Context", max_active: int = 0, max_queue: int = 0, segment_rows: int = 0,
+                 max_inflight_steps: int = 0):
+        cfg = ServerConfig(max_active, max_queue, segment_rows, max_inflight_steps)
+        h = _P()
+        _check(lib().rts_server_start(ctx._h, ctypes.byref(cfg), ctypes.byref(h)), None)
+        self._h = h
+        self.ctx = ctx
+
+    def _c(self, rc):
+        _check(rc, None)
+
+    def submit(self, terms) -> int:
+        arr, n = make_terms(terms)
+        t = ctypes.c_uint64()
+        self._c(lib().rts_server_submit(self._h, arr, n, ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int):
+        done, cnt = ctypes.c_int32(), ctypes.c_uint64()
+        self._c(lib().rts_server_poll(self._h, ticket, ctypes.byref(done), ctypes.byref(cnt)))
+        return bool(done.value), (cnt.value if done.value else None)
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> int:
+        cnt = ctypes.c_uint64()
+        self._c(lib().rts_server_wait(self._h, ticket, timeout_ms, ctypes.byref(cnt)))
+        return cnt.value
+
+    def fetch(self, ticket: int, want_bitmap: bool = True):
+        import numpy as np
+        bm = np.zeros(bitmap_words(self.ctx.nrows), dtype=np.uint32) if want_bitmap else None
+        cnt = ctypes.c_uint64()
+        self._c(lib().rts_server_fetch(self._h, ticket, bm.ctypes.data if bm is not None else None,
+                                       ctypes.byref(cnt)))
+        return bm, cnt.value
+
+    def cancel(self, ticket: int):
+        self._c(lib().rts_server_cancel(self._h, ticket))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._c(lib().rts_server_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def replay(self, queries, arrival_s):
+        """Open-loop replay; returns per-query latency in ms (-1 = rejected)."""
+        import numpy as np
+        pq = queries if isinstance(queries, PreparedQueries) else PreparedQueries(queries)
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        lat = np.zeros(len(pq), dtype=np.float64)
+        self._c(lib().rts_server_replay(self._h, pq.terms, pq.offsets, len(pq),
+                                        arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return lat
+
+    def stop(self):
+        if self._h:
+            h, self._h = self._h, None
+            self._c(lib().rts_server_stop(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 class Context:

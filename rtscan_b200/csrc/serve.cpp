@@ -1,0 +1,619 @@
+// Continuous-batching scan server (rts_server_*).
+//
+// The reference has no serving path: its drivers read a query, scan, check
+// and print, one at a time (bindex_cuda.cpp:1827-1986).  The server keeps
+// the context's columns resident and answers a stream of requests with the
+// batched kernel, as a circular shared scan:
+//
+//   * Memory admission: a pool of `max_active` result slots (one bitmap and
+//     one count each) bounds the requests on the GPU; requests wait in a
+//     bounded queue (RTS_ERR_FULL beyond it) until a slot is free.
+//   * The table is cut into segments of `segment_rows` rows.  Each step
+//     runs the batched kernel over one segment for every active request and
+//     then moves a cursor to the next segment, wrapping around.  A request
+//     admitted while the cursor is at segment c0 has seen every segment once
+//     when the cursor returns to c0; its count, accumulated per segment, and
+//     its bitmap are then final.  New arrivals join at the next step, so
+//     their work overlaps on the device with requests already running.
+//   * The worker thread plans the active set (mask tables) only when it
+//     changes, keeps at most `max_inflight_steps` steps queued on its stream,
+//     and marks a request done when the event recorded after its last step
+//     has completed.
+// Requests the batched kernel does not take (an empty term, no constrained
+// column, more than eight columns) are answered in one launch at admission.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "batch_plan.h"
+#include "rts_internal.h"
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+enum SlotState { FREE = 0, ACTIVE, FINISHING, DONE, CANCELLING };
+
+struct Request {
+  uint64_t ticket;
+  std::vector<rts_term> terms;
+  double t_submit;
+};
+
+}  // namespace
+
+struct rts_server {
+  rts_ctx *ctx = nullptr;
+  rts_server_config cfg{};
+  uint64_t nrows = 0, words = 0, stride = 0, seg_rows = 0;
+  int nseg = 0;
+  uint32_t *bitmaps = nullptr;
+  unsigned long long *counts = nullptr;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+
+  struct PlanBuf {
+    uint32_t *dev = nullptr;
+    size_t cap = 0;
+    uint32_t *host = nullptr;
+    size_t hcap = 0;
+    cudaEvent_t done = nullptr;
+  } pb[2];
+  int next_pb = 0;
+
+  struct Slot {
+    SlotState state = FREE;
+    uint64_t ticket = 0;
+    rts::NormQuery q;
+    int start_seg = 0, segs_done = 0;
+    double t_submit = 0, t_done = 0;
+    cudaEvent_t ev = nullptr;
+    uint64_t count = 0;
+  };
+  std::vector<Slot> slots;
+  std::vector<int> free_slots;
+  std::unordered_map<uint64_t, int> ticket_slot;
+
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request> queue;
+  uint64_t next_ticket = 1;
+  int cursor = 0;
+  uint64_t active_version = 1, plan_version = 0;
+  rts::BatchPlanPtr plan;
+  const uint32_t *plan_dev = nullptr;
+  std::vector<int> plan_slots;
+  std::deque<cudaEvent_t> inflight;
+  std::vector<cudaEvent_t> event_pool;
+
+  // statistics
+  uint64_t submitted = 0, completed = 0, rejected = 0, cancelled = 0, steps = 0;
+  std::vector<double> latencies;
+  std::string fatal;
+  // completions (ticket, done time) for a running replay
+  bool track_done = false;
+  std::vector<std::pair<uint64_t, double>> done_tickets;
+
+  std::atomic<bool> stop{false};
+  std::thread worker;
+
+  cudaEvent_t get_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    RTS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return e;
+  }
+  void put_event(cudaEvent_t e) { event_pool.push_back(e); }
+
+  void upload(const std::vector<uint32_t> &blob) {
+    PlanBuf &b = pb[next_pb];
+    next_pb ^= 1;
+    const size_t bytes = std::max<size_t>(blob.size(), 4) * 4;
+    if (b.done) RTS_CUDA(cudaEventSynchronize(b.done));
+    else RTS_CUDA(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    if (b.cap < bytes) {
+      if (b.dev) cudaFree(b.dev);
+      b.dev = nullptr;
+      b.cap = 0;
+      if (cudaMalloc(&b.dev, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw rts::Error(RTS_ERR_NOMEM, "server plan allocation failed");
+      }
+      b.cap = bytes;
+    }
+    if (b.hcap < bytes) {
+      if (b.host) cudaFreeHost(b.host);
+      b.host = nullptr;
+      RTS_CUDA(cudaMallocHost(&b.host, bytes));
+      b.hcap = bytes;
+    }
+    memcpy(b.host, blob.data(), blob.size() * 4);
+    RTS_CUDA(cudaMemcpyAsync(b.dev, b.host, blob.size() * 4, cudaMemcpyHostToDevice, stream));
+    plan_dev = b.dev;
+    // record the buffer's release after the steps that use it: done at the
+    // next upload into the other buffer, recorded below after each step
+    current_pb = &b;
+  }
+  PlanBuf *current_pb = nullptr;
+
+  // Admit queued requests into free slots (mu held).
+  void admit() {
+    while (!queue.empty() && !free_slots.empty()) {
+      Request r = std::move(queue.front());
+      queue.pop_front();
+      const int sl = free_slots.back();
+      free_slots.pop_back();
+      Slot &S = slots[sl];
+      S.q = rts::normalize(r.terms.data(), (int)r.terms.size(), sl, (int)ctx->cols.size());
+      S.ticket = r.ticket;
+      S.t_submit = r.t_submit;
+      S.segs_done = 0;
+      S.start_seg = cursor;
+      S.count = 0;
+      ticket_slot[r.ticket] = sl;
+      if (!rts::runs_in_kernel(S.q)) {
+        std::vector<rts::NormQuery> one(slots.size());
+        one[sl] = S.q;
+        ctx->launches += rts::launch_outside(ctx, one, {sl}, nullptr, bitmaps, stride, counts, stream);
+        S.ev = get_event();
+        RTS_CUDA(cudaEventRecord(S.ev, stream));
+        S.state = FINISHING;
+      } else {
+        RTS_CUDA(cudaMemsetAsync(counts + sl, 0, 8, stream));
+        S.state = ACTIVE;
+        active_version++;
+      }
+    }
+  }
+
+  void step() {
+    std::vector<int> active;
+    for (size_t i = 0; i < slots.size(); i++)
+      if (slots[i].state == ACTIVE) active.push_back((int)i);
+    if (active.empty()) return;
+    if (plan_version != active_version) {
+      std::vector<rts::NormQuery> norm(slots.size());
+      for (int sl : active) norm[sl] = slots[sl].q;
+      plan = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_table_budget);
+      upload(rts::batch_plan_blob(*plan));
+      plan_version = active_version;
+    }
+    const uint64_t r0 = (uint64_t)cursor * seg_rows;
+    const uint64_t r1 = std::min<uint64_t>(nrows, r0 + seg_rows);
+    ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, stream);
+    RTS_CUDA(cudaGetLastError());
+    cudaEvent_t ev = get_event();
+    RTS_CUDA(cudaEventRecord(ev, stream));
+    inflight.push_back(ev);
+    if (current_pb) RTS_CUDA(cudaEventRecord(current_pb->done, stream));
+    steps++;
+    cursor = (cursor + 1) % nseg;
+    bool changed = false;
+    for (int sl : active) {
+      Slot &S = slots[sl];
+      if (++S.segs_done == nseg) {
+        S.ev = get_event();
+        RTS_CUDA(cudaEventRecord(S.ev, stream));
+        S.state = FINISHING;
+        changed = true;
+      }
+    }
+    if (changed) active_version++;
+  }
+
+  // Mark finished requests done (mu held).
+  void reap() {
+    bool any = false;
+    for (size_t i = 0; i < slots.size(); i++) {
+      Slot &S = slots[i];
+      if (S.state != FINISHING && S.state != CANCELLING) continue;
+      cudaError_t e = cudaEventQuery(S.ev);
+      if (e == cudaErrorNotReady) continue;
+      if (e != cudaSuccess) throw rts::Error(RTS_ERR_CUDA, std::string("server step: ") + cudaGetErrorString(e));
+      put_event(S.ev);
+      S.ev = nullptr;
+      if (S.state == CANCELLING) {
+        S.state = FREE;
+        free_slots.push_back((int)i);
+        continue;
+      }
+      S.state = DONE;
+      S.t_done = now_s();
+      latencies.push_back(S.t_done - S.t_submit);
+      completed++;
+      if (track_done) done_tickets.emplace_back(S.ticket, S.t_done);
+      any = true;
+    }
+    if (any) cv_done.notify_all();
+  }
+
+  void run() {
+    cudaSetDevice(ctx->device);
+    try {
+      while (!stop.load()) {
+        // bound the steps queued on the stream, without holding the lock
+        std::vector<cudaEvent_t> retired;
+        while ((int)inflight.size() >= cfg.max_inflight_steps) {
+          RTS_CUDA(cudaEventSynchronize(inflight.front()));
+          retired.push_back(inflight.front());
+          inflight.pop_front();
+        }
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          for (auto e : retired) put_event(e);
+          admit();
+          reap();
+          bool busy = false;
+          for (auto &S : slots)
+            if (S.state == ACTIVE || S.state == FINISHING || S.state == CANCELLING) busy = true;
+          if (!busy && queue.empty()) {
+            cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            continue;
+          }
+          step();
+        }
+        // let clients in between steps
+        std::this_thread::yield();
+      }
+    } catch (const std::exception &e) {
+      std::lock_guard<std::mutex> lk(mu);
+      fatal = e.what();
+      cv_done.notify_all();
+    }
+  }
+
+  ~rts_server() {
+    stop.store(true);
+    cv_work.notify_all();
+    if (worker.joinable()) worker.join();
+    cudaSetDevice(ctx->device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &b : pb) {
+      if (b.dev) cudaFree(b.dev);
+      if (b.host) cudaFreeHost(b.host);
+      if (b.done) cudaEventDestroy(b.done);
+    }
+    for (auto e : inflight) cudaEventDestroy(e);
+    for (auto e : event_pool) cudaEventDestroy(e);
+    for (auto &S : slots)
+      if (S.ev) cudaEventDestroy(S.ev);
+    if (bitmaps) cudaFree(bitmaps);
+    if (counts) cudaFree(counts);
+    if (stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+  }
+};
+
+namespace {
+
+rts_status fail(rts_server *srv, rts_status code, const std::string &m) {
+  if (srv && srv->ctx) srv->ctx->err = m;
+  return rts::set_thread_error(code, m);
+}
+
+double percentile(std::vector<double> v, double p) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double idx = p * (double)(v.size() - 1);
+  const size_t lo = (size_t)idx, hi = std::min(v.size() - 1, lo + 1);
+  return v[lo] + (v[hi] - v[lo]) * (idx - (double)lo);
+}
+
+}  // namespace
+
+extern "C" {
+
+rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_server **out) {
+  if (!ctx || !out) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (ctx->cols.empty()) return rts::set_thread_error(RTS_ERR_STATE, "no columns loaded");
+  auto *srv = new rts_server();
+  try {
+    srv->ctx = ctx;
+    rts_server_config c{};
+    c.max_active = 512;
+    c.max_queue = 1 << 16;
+    c.segment_rows = 1ull << 22;
+    c.max_inflight_steps = 2;
+    if (cfg) {
+      if (cfg->max_active > 0) c.max_active = cfg->max_active;
+      if (cfg->max_queue > 0) c.max_queue = cfg->max_queue;
+      if (cfg->segment_rows > 0) c.segment_rows = cfg->segment_rows;
+      if (cfg->max_inflight_steps > 0) c.max_inflight_steps = cfg->max_inflight_steps;
+    }
+    if (c.segment_rows % 256) throw rts::Error(RTS_ERR_ARG, "segment_rows must be a multiple of 256");
+    srv->cfg = c;
+    RTS_CUDA(cudaSetDevice(ctx->device));
+    srv->nrows = ctx->nrows;
+    srv->words = rts::words_for(ctx->nrows);
+    srv->stride = (srv->words + 31) / 32 * 32;
+    srv->seg_rows = c.segment_rows;
+    srv->nseg = (int)((srv->nrows + c.segment_rows - 1) / c.segment_rows);
+    const size_t bm_bytes = (size_t)c.max_active * srv->stride * 4;
+    if (cudaMalloc(&srv->bitmaps, bm_bytes) != cudaSuccess || cudaMalloc(&srv->counts, (size_t)c.max_active * 8) != cudaSuccess) {
+      cudaGetLastError();
+      throw rts::Error(RTS_ERR_NOMEM, "result pool of " + std::to_string(bm_bytes) + " bytes does not fit");
+    }
+    RTS_CUDA(cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking));
+    RTS_CUDA(cudaStreamCreateWithFlags(&srv->copy_stream, cudaStreamNonBlocking));
+    srv->slots.resize(c.max_active);
+    for (int i = c.max_active - 1; i >= 0; i--) srv->free_slots.push_back(i);
+    srv->worker = std::thread([srv] { srv->run(); });
+    *out = srv;
+    return RTS_OK;
+  } catch (const rts::Error &e) {
+    delete srv;
+    ctx->err = e.what();
+    return rts::set_thread_error(e.code, e.what());
+  }
+}
+
+rts_status rts_server_submit(rts_server *srv, const rts_term *terms, int32_t nterms, uint64_t *ticket) {
+  if (!srv || !ticket || nterms < 0 || (nterms > 0 && !terms)) return fail(srv, RTS_ERR_ARG, "bad submit arguments");
+  for (int i = 0; i < nterms; i++)
+    if (terms[i].column < 0 || terms[i].column >= (int)srv->ctx->cols.size())
+      return fail(srv, RTS_ERR_ARG, "term column out of range");
+  const double t_submit = now_s();
+  std::lock_guard<std::mutex> lk(srv->mu);
+  if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+  if ((int64_t)srv->queue.size() >= srv->cfg.max_queue) {
+    srv->rejected++;
+    return fail(srv, RTS_ERR_FULL, "request queue full");
+  }
+  Request r;
+  r.ticket = srv->next_ticket++;
+  r.terms.assign(terms, terms + nterms);
+  r.t_submit = t_submit;
+  *ticket = r.ticket;
+  srv->queue.push_back(std::move(r));
+  srv->submitted++;
+  srv->cv_work.notify_one();
+  return RTS_OK;
+}
+
+rts_status rts_server_poll(rts_server *srv, uint64_t ticket, int32_t *done, uint64_t *count) {
+  if (!srv || !done) return fail(srv, RTS_ERR_ARG, "bad poll arguments");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+  *done = 0;
+  auto it = srv->ticket_slot.find(ticket);
+  if (it == srv->ticket_slot.end()) {
+    for (auto &r : srv->queue)
+      if (r.ticket == ticket) return RTS_OK;
+    return fail(srv, RTS_ERR_ARG, "unknown ticket");
+  }
+  rts_server::Slot &S = srv->slots[it->second];
+  if (S.state == DONE) {
+    *done = 1;
+    if (count) {
+      unsigned long long c = 0;
+      cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+      cudaStreamSynchronize(srv->copy_stream);
+      *count = c;
+    }
+  }
+  return RTS_OK;
+}
+
+rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms, uint64_t *count) {
+  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+  std::unique_lock<std::mutex> lk(srv->mu);
+  while (true) {
+    if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+    auto it = srv->ticket_slot.find(ticket);
+    if (it != srv->ticket_slot.end() && srv->slots[it->second].state == DONE) {
+      if (count) {
+        unsigned long long c = 0;
+        cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+        cudaStreamSynchronize(srv->copy_stream);
+        *count = c;
+      }
+      return RTS_OK;
+    }
+    if (it == srv->ticket_slot.end()) {
+      bool queued = false;
+      for (auto &r : srv->queue) queued = queued || r.ticket == ticket;
+      if (!queued) return fail(srv, RTS_ERR_ARG, "unknown ticket");
+    }
+    if (srv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+      auto it2 = srv->ticket_slot.find(ticket);
+      if (it2 != srv->ticket_slot.end() && srv->slots[it2->second].state == DONE) continue;
+      return fail(srv, RTS_ERR_TIMEOUT, "request not done within the timeout");
+    }
+  }
+}
+
+rts_status rts_server_fetch(rts_server *srv, uint64_t ticket, uint32_t *host_bitmap, uint64_t *count) {
+  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->ticket_slot.find(ticket);
+  if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown or unfinished ticket");
+  const int sl = it->second;
+  rts_server::Slot &S = srv->slots[sl];
+  if (S.state != DONE) return fail(srv, RTS_ERR_STATE, "request not done");
+  cudaError_t e = cudaSuccess;
+  if (host_bitmap)
+    e = cudaMemcpyAsync(host_bitmap, srv->bitmaps + (uint64_t)sl * srv->stride, srv->words * 4,
+                        cudaMemcpyDeviceToHost, srv->copy_stream);
+  unsigned long long c = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&c, srv->counts + sl, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(srv->copy_stream);
+  if (e != cudaSuccess) return fail(srv, RTS_ERR_CUDA, std::string("fetch: ") + cudaGetErrorString(e));
+  if (count) *count = c;
+  S.state = FREE;
+  srv->ticket_slot.erase(it);
+  srv->free_slots.push_back(sl);
+  srv->cv_work.notify_one();
+  return RTS_OK;
+}
+
+rts_status rts_server_cancel(rts_server *srv, uint64_t ticket) {
+  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  for (auto it = srv->queue.begin(); it != srv->queue.end(); ++it)
+    if (it->ticket == ticket) {
+      srv->queue.erase(it);
+      srv->cancelled++;
+      return RTS_OK;
+    }
+  auto it = srv->ticket_slot.find(ticket);
+  if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown ticket");
+  rts_server::Slot &S = srv->slots[it->second];
+  if (S.state == ACTIVE) {
+    // kernels already queued may still write this slot: free it after them
+    S.ev = srv->get_event();
+    cudaEventRecord(S.ev, srv->stream);
+    S.state = CANCELLING;
+    srv->active_version++;
+  } else if (S.state == FINISHING) {
+    S.state = CANCELLING;
+  } else if (S.state == DONE) {
+    S.state = FREE;
+    srv->free_slots.push_back(it->second);
+  }
+  srv->ticket_slot.erase(it);
+  srv->cancelled++;
+  return RTS_OK;
+}
+
+rts_status rts_server_get_stats(rts_server *srv, rts_server_stats *st) {
+  if (!srv || !st) return fail(srv, RTS_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(srv->mu);
+  memset(st, 0, sizeof *st);
+  st->submitted = srv->submitted;
+  st->completed = srv->completed;
+  st->rejected = srv->rejected;
+  st->cancelled = srv->cancelled;
+  st->steps = srv->steps;
+  st->queued = srv->queue.size();
+  int active = 0;
+  for (auto &S : srv->slots) active += S.state == ACTIVE;
+  st->active = (uint32_t)active;
+  st->p50_ms = percentile(srv->latencies, 0.50) * 1e3;
+  st->p99_ms = percentile(srv->latencies, 0.99) * 1e3;
+  st->p999_ms = percentile(srv->latencies, 0.999) * 1e3;
+  double mx = 0, sum = 0;
+  for (double v : srv->latencies) {
+    mx = std::max(mx, v);
+    sum += v;
+  }
+  st->max_ms = mx * 1e3;
+  st->mean_ms = srv->latencies.empty() ? 0 : sum / (double)srv->latencies.size() * 1e3;
+  return RTS_OK;
+}
+
+rts_status rts_server_stop(rts_server *srv) {
+  if (!srv) return RTS_OK;
+  std::string fatal;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    fatal = srv->fatal;
+  }
+  delete srv;
+  if (!fatal.empty()) return rts::set_thread_error(RTS_ERR_CUDA, "server had stopped: " + fatal);
+  return RTS_OK;
+}
+
+// Open-loop replay for benchmarks: request q is submitted at arrival_s[q]
+// seconds after the call starts, and its result slot is released as soon
+// as it is done.  latency_ms[q] receives submit-to-done time (or -1 when
+// the queue was full).  Blocks until every request is done.
+rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets, int32_t nq,
+                             const double *arrival_s, double *latency_ms) {
+  if (!srv || nq < 0 || (nq > 0 && (!offsets || !arrival_s || !latency_ms)))
+    return fail(srv, RTS_ERR_ARG, "bad replay arguments");
+  std::unordered_map<uint64_t, int> index_of;  // ticket -> query, filled by the producer
+  std::vector<double> t_sub(nq, 0);
+  std::atomic<int> produced{0};
+  std::atomic<int> rejected{0};
+  rts_status prod_err = RTS_OK;
+  std::mutex map_mu;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->track_done = true;
+    srv->done_tickets.clear();
+  }
+  const double t0 = now_s();
+  std::thread producer([&] {
+    for (int q = 0; q < nq; q++) {
+      const double due = t0 + arrival_s[q];
+      while (now_s() < due) {
+        const double left = due - now_s();
+        if (left > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(left * 5e5)));
+      }
+      t_sub[q] = now_s();
+      uint64_t tk = 0;
+      std::lock_guard<std::mutex> ml(map_mu);  // the consumer may look the ticket up right away
+      const rts_status rc = rts_server_submit(srv, terms + offsets[q], offsets[q + 1] - offsets[q], &tk);
+      if (rc == RTS_ERR_FULL) {
+        latency_ms[q] = -1;
+        rejected++;
+      } else if (rc != RTS_OK) {
+        prod_err = rc;
+        produced.store(nq);
+        return;
+      } else {
+        index_of[tk] = q;
+      }
+      produced.store(q + 1);
+    }
+  });
+  // consumer: release every finished request as it completes
+  int finished = 0;
+  rts_status rc = RTS_OK;
+  while (rc == RTS_OK) {
+    std::vector<std::pair<uint64_t, double>> batch;
+    {
+      std::unique_lock<std::mutex> lk(srv->mu);
+      if (srv->done_tickets.empty()) srv->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+      if (!srv->fatal.empty()) {
+        rc = RTS_ERR_CUDA;
+        break;
+      }
+      batch.swap(srv->done_tickets);
+    }
+    for (auto &d : batch) {
+      int q;
+      {
+        std::lock_guard<std::mutex> ml(map_mu);
+        auto it = index_of.find(d.first);
+        if (it == index_of.end()) continue;  // not one of this replay's requests
+        q = it->second;
+        index_of.erase(it);
+      }
+      rc = rts_server_fetch(srv, d.first, nullptr, nullptr);
+      if (rc != RTS_OK) break;
+      latency_ms[q] = (d.second - t_sub[q]) * 1e3;
+      finished++;
+    }
+    if (prod_err != RTS_OK) rc = prod_err;
+    if (produced.load() == nq && finished + rejected.load() == nq) break;
+  }
+  producer.join();
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->track_done = false;
+    srv->done_tickets.clear();
+  }
+  if (rc == RTS_OK) rc = prod_err;
+  if (rc != RTS_OK && rc != RTS_ERR_CUDA) return rc;
+  if (rc == RTS_ERR_CUDA) return fail(srv, rc, "server stopped: " + srv->fatal);
+  return RTS_OK;
+}
+
+}  // extern "C"
