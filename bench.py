@@ -263,6 +263,9 @@ def run(args):
     out = torch.empty(nq * stride, dtype=torch.int32, device=dev)
     cnt = torch.zeros(nq, dtype=torch.int64, device=dev)
     bytes_step = step_bytes(n, queries)
+    tuned = None
+    if wl == "batched" and not args.no_autotune:
+        tuned = ctx.autotune_batch(pq)  # launch shape for this table and batch (outside the timed region)
     if wl == "batched":
         launch = lambda: ctx.scan_batch_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s)
     else:
@@ -385,7 +388,23 @@ def run(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if wl == "batched":
+        line["batch_config"] = ctx.batch_config()
+        line["batch_config"]["source"] = "autotuned" if tuned else "default"
     line.update(extra)
+
+    if wl == "batched" and not args.no_serve:
+        del out, cnt
+        ctx.attach_columns([c.data_ptr() for c in cols[:1]], n)
+        del cols
+        torch.cuda.empty_cache()
+        line["served"] = served_leg(torch, R, D, ctx, dev, rank, args)
+        rates = line["served"]["rates"]
+        ref = min(rates, key=lambda r: abs(r["offered_qps"] - 5000)) if rates else None
+        if ref:
+            line["served_p50_ms"] = ref["p50_ms"]
+            line["served_p99_ms"] = ref["p99_ms"]
+            line["served_at_qps"] = ref["offered_qps"]
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cols_np = cpu_sample_columns(kinds, REF_N)
@@ -403,6 +422,49 @@ def run(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+SERVE_KINDS = ["uniform", "uniform", "zipf1.3", "zipf1.3"]
+
+
+def served_leg(torch, R, D, ctx, dev, rank, args):
+    """Served scan: a resident 2^28-row x 4-column table
+    (2 uniform + 2 zipf 1.3 columns, 4 GiB), open-loop Poisson arrivals at
+    several rates of queries over 1-4 columns with log-uniform selectivity,
+    answered by the continuous-batching server; plus a burst of 256
+    concurrent 4-column queries.  Latency is submit-to-done per request."""
+    n = args.serve_rows
+    cols = [gpu_column(torch, k, n, 5000 * (rank + 1) + i, dev) for i, k in enumerate(SERVE_KINDS)]
+    ctx.attach_columns([c.data_ptr() for c in cols], n)
+    samples = [host_sample(torch, c, seed=11 + i) for i, c in enumerate(cols)]
+    out = {"table": f"{n} rows x {len(cols)} columns ({', '.join(SERVE_KINDS)})", "segment_rows": 1 << 23,
+           "max_active": 1024, "rates": []}
+    seconds = args.serve_seconds
+    with R.Server(ctx, max_active=1024, segment_rows=1 << 23) as srv:
+        # warm-up
+        srv.replay(D.batch_queries(samples, 200, seed=1), np.linspace(0, 0.05, 200))
+        for rate in args.serve_rates:
+            nq = max(1, int(rate * seconds))
+            qs = R.prepare(D.batch_queries(samples, nq, seed=rate))
+            arr = np.cumsum(np.random.default_rng(rate).exponential(1.0 / rate, size=nq))
+            t0 = time.perf_counter()
+            lat = srv.replay(qs, arr)
+            wall = time.perf_counter() - t0
+            ok = lat[lat >= 0]
+            out["rates"].append({"offered_qps": rate, "queries": nq, "achieved_qps": round(len(ok) / wall, 1),
+                                 "rejected": int((lat < 0).sum()),
+                                 "p50_ms": round(float(np.percentile(ok, 50)), 3),
+                                 "p99_ms": round(float(np.percentile(ok, 99)), 3),
+                                 "p999_ms": round(float(np.percentile(ok, 99.9)), 3)})
+        q4 = R.prepare(D.batch_queries(samples, 256, seed=4, min_cols=4, max_cols=4))
+        t0 = time.perf_counter()
+        lat = srv.replay(q4, np.zeros(256))
+        wall = time.perf_counter() - t0
+        out["burst_256x4col"] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
+                                 "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                                 "qps": round(256 / wall, 1)}
+    del cols
+    return out
 
 
 def run_reference(args):
@@ -455,6 +517,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-compare", action="store_true", help="skip the one-query-per-launch comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-scan leg")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default batch launch shape")
+    ap.add_argument("--serve-rows", type=int, default=1 << 28)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[1000, 5000, 10000])
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

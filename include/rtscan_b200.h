@@ -235,6 +235,22 @@ RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, cons
                                        int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
                                        uint64_t *dev_counts, void *stream);
 
+/* ---- batched-kernel launch shape and its autotuner ------------------------ */
+typedef struct rts_batch_config {
+  int32_t warps_per_cta;        /* 8 or 16 (each warp stages 8 KiB of result words) */
+  int32_t max_queries_per_pass; /* 1..256 */
+  uint32_t table_budget_bytes;  /* shared memory a pass may use for its mask tables, 4..160 KiB */
+} rts_batch_config;
+RTS_API rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg);
+RTS_API rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg);
+/* Time every candidate launch shape on a row sample (up to 2^24 rows) of the
+ * resident table with these queries, keep the fastest for this context, and
+ * report it in *best (may be NULL).  With a cache_path, a previous result for
+ * the same GPU, SM count, column count, table size and batch size is reused
+ * and new results are appended. */
+RTS_API rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
+                                      int32_t nqueries, const char *cache_path, rts_batch_config *best);
+
 /* ---- serving: continuous batching over resident columns ----------------- */
 /* No reference counterpart (the reference drivers answer one query at a time,
  * bindex_cuda.cpp:1827-1986).  A server owns a worker thread that runs the

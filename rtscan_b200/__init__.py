@@ -49,6 +49,15 @@ class ServerConfig(ctypes.Structure):
                 ("max_inflight_steps", ctypes.c_int32)]
 
 
+class BatchConfig(ctypes.Structure):
+    """rts_batch_config: launch shape of the batched kernel."""
+    _fields_ = [("warps_per_cta", ctypes.c_int32), ("max_queries_per_pass", ctypes.c_int32),
+                ("table_budget_bytes", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("cancelled", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("queued", ctypes.c_uint64),
@@ -109,6 +118,10 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_set_batch_config", ctypes.c_int32, [_P, ctypes.POINTER(BatchConfig)]),
+    ("rts_get_batch_config", ctypes.c_int32, [_P, ctypes.POINTER(BatchConfig)]),
+    ("rts_autotune_batch", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
+                                            ctypes.c_char_p, ctypes.POINTER(BatchConfig)]),
     ("rts_server_start", ctypes.c_int32, [_P, ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
     ("rts_server_submit", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, _U64P]),
     ("rts_server_poll", ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), _U64P]),
@@ -434,6 +447,22 @@ class Context:
         self._c(lib().rts_scan_batch_host(self._h, ptrs, len(host_cols), n, arr, off, len(queries),
                                           host_bitmaps.ctypes.data, stride, counts.ctypes.data))
         return host_bitmaps, counts
+
+    def batch_config(self) -> dict:
+        c = BatchConfig()
+        self._c(lib().rts_get_batch_config(self._h, ctypes.byref(c)))
+        return c.as_dict()
+
+    def set_batch_config(self, warps_per_cta: int, max_queries_per_pass: int, table_budget_bytes: int):
+        c = BatchConfig(warps_per_cta, max_queries_per_pass, table_budget_bytes)
+        self._c(lib().rts_set_batch_config(self._h, ctypes.byref(c)))
+
+    def autotune_batch(self, queries, cache_path: Optional[str] = None) -> dict:
+        arr, off = self._csr(queries)
+        c = BatchConfig()
+        self._c(lib().rts_autotune_batch(self._h, arr, off, len(queries),
+                                         cache_path.encode() if cache_path else None, ctypes.byref(c)))
+        return c.as_dict()
 
     def bitmap_op_async(self, op: int, dst: int, a: int, b: int, words: int, value: int = 0, stream: int = 0):
         self._c(lib().rts_bitmap_op_async(self._h, op, dst, a, b, words, value, stream))

@@ -44,8 +44,6 @@ constexpr int kSlots = 256;         // queries per pass
 constexpr int kGroups = kSlots / 32;
 constexpr int kMaxCols = 8;         // constrained columns per pass
 constexpr int kTilesPerBlock = 8;   // 8 tiles x 32 rows = one 32-byte sector per query
-constexpr int kWarps = 16;
-constexpr int kThreads = kWarps * 32;
 constexpr int kStageWords = kSlots * kTilesPerBlock;  // per warp
 template <int CMAX>
 constexpr int kPosWords = 36 * CMAX;  // per warp: 32 rows + one padding row per 8
@@ -125,15 +123,16 @@ __device__ __forceinline__ uint32_t stage_index(uint32_t slot, uint32_t t) {
   return row * 32 + col;
 }
 
-template <int CMAX>
-__global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constant__ BatchPass p) {
+// CMAX: columns a pass may constrain (4 or 8); W: warps per CTA (8 or 16).
+template <int CMAX, int W>
+__global__ void __launch_bounds__(W * 32, 16 / W) batch_kernel(const __grid_constant__ BatchPass p) {
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t *blob = smem;
   uint32_t *stage_all = smem + ((p.blob_words + 3) & ~3u);
   // positions of a warp's 32-row tile: row r at r*CMAX + (r/8)*CMAX words,
   // so the four rows read together (s*8+i, s = 0..3) sit in different banks
-  uint32_t *posbuf_all = stage_all + kWarps * kStageWords;
-  unsigned int *cta_count = posbuf_all + kWarps * kPosWords<CMAX>;
+  uint32_t *posbuf_all = stage_all + W * kStageWords;
+  unsigned int *cta_count = posbuf_all + W * kPosWords<CMAX>;
 
   for (uint32_t i = threadIdx.x; i < p.blob_words; i += blockDim.x) blob[i] = __ldg(p.blob + i);
   for (int i = threadIdx.x; i < kSlots; i += blockDim.x) cta_count[i] = 0;
@@ -153,8 +152,8 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
 #pragma unroll
   for (int k = 0; k < 8; k++) cnt[k] = 0;
 
-  const uint64_t gwarp = (uint64_t)blockIdx.x * kWarps + warp;
-  const uint64_t nwarps = (uint64_t)gridDim.x * kWarps;
+  const uint64_t gwarp = (uint64_t)blockIdx.x * W + warp;
+  const uint64_t nwarps = (uint64_t)gridDim.x * W;
   for (uint64_t blk = p.block_begin + gwarp; blk < p.nblocks; blk += nwarps) {
     const uint64_t row0 = blk * (32 * kTilesPerBlock);
     // every column value of the block, loaded up front (lane = row in tile)
@@ -282,23 +281,32 @@ __global__ void __launch_bounds__(kThreads, 1) batch_kernel(const __grid_constan
   }
 }
 
-template <int CMAX>
+template <int CMAX, int W>
 size_t smem_bytes(uint32_t blob_words) {
-  return ((blob_words + 3) & ~3u) * 4 + (size_t)kWarps * kStageWords * 4 + (size_t)kWarps * kPosWords<CMAX> * 4 +
-         kSlots * 4;
+  return ((blob_words + 3) & ~3u) * 4 + (size_t)W * kStageWords * 4 + (size_t)W * kPosWords<CMAX> * 4 + kSlots * 4;
 }
 
-template <int CMAX>
+template <int CMAX, int W>
 int blocks_per_sm(size_t smem) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(batch_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(batch_kernel<CMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     attr_set = true;
   }
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<CMAX>, kThreads, smem) != cudaSuccess || b < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<CMAX, W>, W * 32, smem) != cudaSuccess ||
+      b < 1)
     b = 1;
   return b;
+}
+
+template <int CMAX, int W>
+void launch_one(const BatchPass &bp, int sm_count, cudaStream_t s) {
+  const size_t sm = smem_bytes<CMAX, W>(bp.blob_words);
+  const int per = blocks_per_sm<CMAX, W>(sm);
+  const uint64_t want = (bp.nblocks - bp.block_begin + W - 1) / W;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per * sm_count));
+  batch_kernel<CMAX, W><<<grid, W * 32, sm, s>>>(bp);
 }
 
 }  // namespace
@@ -352,8 +360,8 @@ size_t column_bytes(size_t m) {
 }
 
 // Add query q to the pass if its tables still fit the budget.
-bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget) {
-  if ((int)pp.qs.size() >= kSlots) return false;
+bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_per_pass) {
+  if ((int)pp.qs.size() >= std::min(max_per_pass, kSlots)) return false;
   size_t total = 0;
   int new_cols = 0;
   std::vector<size_t> grow(pp.cols.size(), 0);
@@ -477,9 +485,10 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
                      const int32_t *out_index, size_t table_budget) {
   std::vector<PassPlan> passes;
   for (int qi : which) {
-    if (passes.empty() || !try_add(passes.back(), norm[qi], qi, table_budget)) {
+    const int per = ctx->batch_cfg.max_queries_per_pass;
+    if (passes.empty() || !try_add(passes.back(), norm[qi], qi, table_budget, per)) {
       passes.emplace_back();
-      if (!try_add(passes.back(), norm[qi], qi, table_budget))
+      if (!try_add(passes.back(), norm[qi], qi, table_budget, per))
         throw Error(RTS_ERR_ARG, "query does not fit one batch pass");
     }
   }
@@ -593,17 +602,13 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.block_begin = row_begin / rows_per_block;
     bp.nblocks = (row_end + rows_per_block - 1) / rows_per_block;
     bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
-    const uint64_t want = (bp.nblocks - bp.block_begin + kWarps - 1) / kWarps;
+    const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
     if (b.cmax == 4) {
-      const size_t sm = smem_bytes<4>(bp.blob_words);
-      const int per = blocks_per_sm<4>(sm);
-      const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per * ctx->sm_count));
-      batch_kernel<4><<<grid, kThreads, sm, s>>>(bp);
+      if (w8) launch_one<4, 8>(bp, ctx->sm_count, s);
+      else launch_one<4, 16>(bp, ctx->sm_count, s);
     } else {
-      const size_t sm = smem_bytes<8>(bp.blob_words);
-      const int per = blocks_per_sm<8>(sm);
-      const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per * ctx->sm_count));
-      batch_kernel<8><<<grid, kThreads, sm, s>>>(bp);
+      if (w8) launch_one<8, 8>(bp, ctx->sm_count, s);
+      else launch_one<8, 16>(bp, ctx->sm_count, s);
     }
     launches++;
   }
@@ -777,7 +782,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       std::vector<int32_t> off(offsets + q0, offsets + q1 + 1);
       for (auto &o : off) o -= offsets[q0];
       rts::batch_scan(ctx, terms + offsets[q0], off.data(), q1 - q0, H.bitmaps + (uint64_t)q0 * stride_words,
-                      stride_words, H.counts + q0, H.compute, ctx->batch_table_budget);
+                      stride_words, H.counts + q0, H.compute, ctx->batch_cfg.table_budget);
       RTS_CUDA(cudaEventRecord(H.ev[k], H.compute));
       RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[k], 0));
       RTS_CUDA(cudaMemcpyAsync(host_bitmaps + (uint64_t)q0 * stride_words, H.bitmaps + (uint64_t)q0 * stride_words,
@@ -812,7 +817,8 @@ extern "C" rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, 
     cudaGetDevice(&prev);
     if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
     rts::batch_scan(ctx, terms, offsets, nq, dev_bitmaps, stride_words,
-                    reinterpret_cast<unsigned long long *>(dev_counts), (cudaStream_t)stream, ctx->batch_table_budget);
+                    reinterpret_cast<unsigned long long *>(dev_counts), (cudaStream_t)stream,
+                    ctx->batch_cfg.table_budget);
     if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {

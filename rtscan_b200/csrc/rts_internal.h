@@ -100,9 +100,14 @@ struct BatchScratch;
 void destroy_batch(BatchScratch *b);
 struct HostBatchBuffers;
 void destroy_host_batch(HostBatchBuffers *b);
-// Shared-memory bytes one batch pass may spend on its mask tables; the
-// rest of the CTA's shared memory stages result words.
-constexpr size_t kDefaultBatchTableBudget = 88 * 1024;
+// Launch shape of the batched kernel: warps per CTA (8 or 16), queries per
+// pass (<= 256) and the shared-memory bytes a pass may spend on its mask
+// tables (the rest of the CTA's shared memory stages result words).
+struct BatchConfig {
+  int warps_per_cta = 16;
+  int max_queries_per_pass = 256;
+  size_t table_budget = 88 * 1024;
+};
 void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq, uint32_t *out,
                 uint64_t stride_words, unsigned long long *counts, cudaStream_t s, size_t table_budget);
 
@@ -127,7 +132,7 @@ struct rts_ctx {
   void *small_dev = nullptr;
   rts::BatchScratch *batch = nullptr;
   rts::HostBatchBuffers *host_batch = nullptr;
-  size_t batch_table_budget = rts::kDefaultBatchTableBudget;
+  rts::BatchConfig batch_cfg;
   std::atomic<uint64_t> launches{0};
   std::string err;
   ~rts_ctx();

@@ -188,7 +188,7 @@ struct rts_server {
     if (plan_version != active_version) {
       std::vector<rts::NormQuery> norm(slots.size());
       for (int sl : active) norm[sl] = slots[sl].q;
-      plan = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_table_budget);
+      plan = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget);
       upload(rts::batch_plan_blob(*plan));
       plan_version = active_version;
     }

@@ -1,0 +1,176 @@
+// Autotuner for the batched kernel's launch shape.
+//
+// The batched kernel's speed depends on three knobs that trade shared memory
+// against each other: warps per CTA (each warp stages 8 KB of result words),
+// queries per pass (more queries share each row's interval lookups but need
+// larger mask tables) and the mask-table budget (which fixes how many
+// queries fit a pass and how many CTAs fit an SM).  rts_autotune_batch runs
+// every candidate on a row sample of the resident table with the caller's
+// queries, keeps the fastest, and can cache the choice in a small text file
+// keyed by GPU, SM count, column count, table size and batch size.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "rts_internal.h"
+
+namespace {
+
+struct Candidate {
+  int warps, qpp;
+  size_t budget;
+};
+
+const Candidate kCandidates[] = {
+    {16, 256, 88 * 1024}, {16, 256, 64 * 1024}, {16, 128, 88 * 1024},
+    {8, 256, 40 * 1024},  {8, 128, 40 * 1024},  {8, 256, 140 * 1024},
+};
+
+std::string cache_key(rts_ctx *ctx, int nq) {
+  cudaDeviceProp p;
+  std::string name = "gpu";
+  if (cudaGetDeviceProperties(&p, ctx->device) == cudaSuccess) name = p.name;
+  for (auto &ch : name)
+    if (ch == ' ' || ch == '|') ch = '_';
+  int lg = 0;
+  while ((1ull << (lg + 1)) <= ctx->nrows) lg++;
+  int qb = 1;
+  while (qb < nq) qb <<= 1;
+  return name + "|" + std::to_string(ctx->sm_count) + "|" + std::to_string(ctx->cols.size()) + "|" +
+         std::to_string(lg) + "|" + std::to_string(qb);
+}
+
+bool cache_lookup(const char *path, const std::string &key, rts::BatchConfig *out) {
+  if (!path) return false;
+  FILE *f = fopen(path, "r");
+  if (!f) return false;
+  char line[512];
+  bool found = false;
+  while (fgets(line, sizeof line, f)) {
+    char k[400];
+    int w, q;
+    unsigned long b;
+    double ms;
+    if (sscanf(line, "%399s %d %d %lu %lf", k, &w, &q, &b, &ms) == 5 && key == k) {
+      out->warps_per_cta = w;
+      out->max_queries_per_pass = q;
+      out->table_budget = b;
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void cache_store(const char *path, const std::string &key, const rts::BatchConfig &c, double ms) {
+  if (!path) return;
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d %lu %.4f\n", key.c_str(), c.warps_per_cta, c.max_queries_per_pass,
+          (unsigned long)c.table_budget, ms);
+  fclose(f);
+}
+
+bool valid(const rts_batch_config &c) {
+  return (c.warps_per_cta == 8 || c.warps_per_cta == 16) && c.max_queries_per_pass >= 1 &&
+         c.max_queries_per_pass <= 256 && c.table_budget_bytes >= 4096 && c.table_budget_bytes <= 160 * 1024;
+}
+
+}  // namespace
+
+extern "C" {
+
+rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg) {
+  if (!ctx || !cfg) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
+  if (!valid(*cfg)) {
+    ctx->err = "batch config out of range (warps 8|16, 1..256 queries per pass, 4..160 KiB table budget)";
+    return rts::set_thread_error(RTS_ERR_ARG, ctx->err);
+  }
+  ctx->batch_cfg.warps_per_cta = cfg->warps_per_cta;
+  ctx->batch_cfg.max_queries_per_pass = cfg->max_queries_per_pass;
+  ctx->batch_cfg.table_budget = cfg->table_budget_bytes;
+  return RTS_OK;
+}
+
+rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg) {
+  if (!ctx || !cfg) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
+  cfg->warps_per_cta = ctx->batch_cfg.warps_per_cta;
+  cfg->max_queries_per_pass = ctx->batch_cfg.max_queries_per_pass;
+  cfg->table_budget_bytes = (uint32_t)ctx->batch_cfg.table_budget;
+  return RTS_OK;
+}
+
+rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
+                              const char *cache_path, rts_batch_config *best_out) {
+  if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
+  if (ctx->cols.empty()) return rts::set_thread_error(RTS_ERR_STATE, "no columns loaded");
+  if (nq < 1 || !offsets) return rts::set_thread_error(RTS_ERR_ARG, "need at least one query");
+  const std::string key = cache_key(ctx, nq);
+  rts::BatchConfig cached;
+  if (cache_lookup(cache_path, key, &cached)) {
+    ctx->batch_cfg = cached;
+    if (best_out) rts_get_batch_config(ctx, best_out);
+    return RTS_OK;
+  }
+  const uint64_t saved_n = ctx->nrows;
+  const rts::BatchConfig saved_cfg = ctx->batch_cfg;
+  uint32_t *bm = nullptr;
+  unsigned long long *cnt = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  rts_status rc = RTS_OK;
+  try {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    // tune on a row sample (all of a small table)
+    const uint64_t sample = std::min<uint64_t>(saved_n, 1ull << 24);
+    ctx->nrows = sample;
+    const uint64_t stride = (rts::words_for(sample) + 31) / 32 * 32;
+    if (cudaMalloc(&bm, (size_t)nq * stride * 4) != cudaSuccess || cudaMalloc(&cnt, (size_t)nq * 8) != cudaSuccess) {
+      cudaGetLastError();
+      throw rts::Error(RTS_ERR_NOMEM, "autotune buffers do not fit");
+    }
+    RTS_CUDA(cudaEventCreate(&e0));
+    RTS_CUDA(cudaEventCreate(&e1));
+    double best_ms = 1e300;
+    rts::BatchConfig best = saved_cfg;
+    for (const Candidate &c : kCandidates) {
+      ctx->batch_cfg.warps_per_cta = c.warps;
+      ctx->batch_cfg.max_queries_per_pass = c.qpp;
+      ctx->batch_cfg.table_budget = c.budget;
+      rts::batch_scan(ctx, terms, offsets, nq, bm, stride, cnt, nullptr, c.budget);  // warm-up
+      RTS_CUDA(cudaEventRecord(e0, nullptr));
+      for (int r = 0; r < 2; r++) rts::batch_scan(ctx, terms, offsets, nq, bm, stride, cnt, nullptr, c.budget);
+      RTS_CUDA(cudaEventRecord(e1, nullptr));
+      RTS_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      RTS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms / 2 < best_ms) {
+        best_ms = ms / 2;
+        best = ctx->batch_cfg;
+      }
+    }
+    ctx->batch_cfg = best;
+    ctx->nrows = saved_n;
+    cache_store(cache_path, key, best, best_ms);
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+  } catch (const rts::Error &e) {
+    ctx->nrows = saved_n;
+    ctx->batch_cfg = saved_cfg;
+    ctx->err = e.what();
+    rc = rts::set_thread_error(e.code, e.what());
+  }
+  if (bm) cudaFree(bm);
+  if (cnt) cudaFree(cnt);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc == RTS_OK && best_out) rts_get_batch_config(ctx, best_out);
+  return rc;
+}
+
+}  // extern "C"

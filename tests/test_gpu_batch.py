@@ -127,3 +127,34 @@ def test_batch_alone_and_in_the_mix(ctx):
         alone = run_batch(ctx, [qs[i]])[0]
         assert alone[1] == mixed[i][1]
         assert np.array_equal(alone[0], mixed[i][0])
+
+
+@pytest.mark.parametrize("cfg", [(16, 256, 88 * 1024), (16, 64, 16 * 1024), (8, 256, 40 * 1024),
+                                 (8, 128, 140 * 1024), (8, 1, 4096)])
+def test_batch_every_launch_shape(ctx, cfg):
+    n = 150_011
+    cols = [D.uniform(n, 200), D.zipf(n, 201, 1.1), D.uniform(n, 202, 1000), D.normal(n, 203)]
+    ctx.load_columns(cols)
+    old = ctx.batch_config()
+    ctx.set_batch_config(*cfg)
+    try:
+        check_batch(ctx, cols, D.batch_queries(cols, 300, seed=cfg[1]))
+    finally:
+        ctx.set_batch_config(old["warps_per_cta"], old["max_queries_per_pass"], old["table_budget_bytes"])
+
+
+def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
+    n = 1 << 20
+    cols = [D.zipf(n, 210, 1.3), D.normal(n, 211)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 200, seed=4)
+    cache = str(tmp_path / "tune.txt")
+    best = ctx.autotune_batch(qs, cache)
+    assert best["warps_per_cta"] in (8, 16)
+    assert 1 <= best["max_queries_per_pass"] <= 256
+    assert open(cache).read().strip()
+    again = ctx.autotune_batch(qs, cache)  # served from the cache
+    assert again == best
+    check_batch(ctx, cols, qs)
+    with pytest.raises(R.RtsError):
+        ctx.set_batch_config(12, 256, 88 * 1024)
