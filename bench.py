@@ -313,6 +313,16 @@ def run(args):
         sep_ms = statistics.median(per_sep)
         extra["separate_passes_ms"] = round(sep_ms, 4)
         extra["fused_speedup_vs_separate"] = round(sep_ms / statistics.median(per), 3)
+    if wl == "batched":
+        # the same batch prepared once and replayed as one CUDA graph per step
+        pb = ctx.prepare_batch(pq, out.data_ptr(), stride, cnt.data_ptr())
+        pb.launch(s)
+        per_g, _ = timed(lambda: pb.launch(s), args.steps)
+        extra["graph_replay_ms_per_step"] = round(statistics.median(per_g), 4)
+        pb.release()
+    if world > 1:
+        from rtscan_b200 import shard as SH
+        extra["global_match_count_q0"] = int(SH.all_reduce_counts(cnt[:1].cpu().numpy())[0])
     if wl == "batched" and not args.no_compare:
         each = lambda: ctx.scan_each_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s)
         each()

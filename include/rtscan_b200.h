@@ -235,6 +235,19 @@ RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, cons
                                        int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
                                        uint64_t *dev_counts, void *stream);
 
+/* ---- prepared batches (CUDA graphs) -------------------------------------- */
+typedef struct rts_prepared rts_prepared;
+/* Plan a batch once and capture all of its launches (count reset, fills,
+ * fused launches, one batched kernel per pass) into a CUDA graph writing
+ * dev_bitmaps / dev_counts as rts_scan_batch_async would.  Re-prepare after
+ * reloading the table. */
+RTS_API rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
+                                     int32_t nqueries, uint32_t *dev_bitmaps, uint64_t stride_words,
+                                     uint64_t *dev_counts, rts_prepared **out);
+/* Replay a prepared batch on `stream` (one graph launch). */
+RTS_API rts_status rts_batch_launch(rts_prepared *p, void *stream);
+RTS_API void rts_batch_release(rts_prepared *p);
+
 /* ---- batched-kernel launch shape and its autotuner ------------------------ */
 typedef struct rts_batch_config {
   int32_t warps_per_cta;        /* 8 or 16 (each warp stages 8 KiB of result words) */

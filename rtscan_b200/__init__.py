@@ -118,6 +118,10 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_batch_prepare", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P,
+                                           ctypes.c_uint64, _P, ctypes.POINTER(_P)]),
+    ("rts_batch_launch", ctypes.c_int32, [_P, _P]),
+    ("rts_batch_release", None, [_P]),
     ("rts_set_batch_config", ctypes.c_int32, [_P, ctypes.POINTER(BatchConfig)]),
     ("rts_get_batch_config", ctypes.c_int32, [_P, ctypes.POINTER(BatchConfig)]),
     ("rts_autotune_batch", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
@@ -249,6 +253,28 @@ class PreparedQueries:
 
 def prepare(queries) -> PreparedQueries:
     return PreparedQueries(queries)
+
+
+class PreparedBatch:
+    """A batch replayed as one CUDA graph launch (rts_batch_prepare)."""
+
+    def __init__(self, ctx, h):
+        self.ctx = ctx
+        self._h = h
+
+    def launch(self, stream: int = 0):
+        _check(lib().rts_batch_launch(self._h, stream), self.ctx._h)
+
+    def release(self):
+        if self._h:
+            lib().rts_batch_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 class Server:
@@ -447,6 +473,14 @@ class Context:
         self._c(lib().rts_scan_batch_host(self._h, ptrs, len(host_cols), n, arr, off, len(queries),
                                           host_bitmaps.ctypes.data, stride, counts.ctypes.data))
         return host_bitmaps, counts
+
+    def prepare_batch(self, queries, bitmaps_ptr: int, stride_words: int, counts_ptr: int) -> "PreparedBatch":
+        """Plan `queries` once and capture their launches in a CUDA graph."""
+        arr, off = self._csr(queries)
+        h = _P()
+        self._c(lib().rts_batch_prepare(self._h, arr, off, len(queries), bitmaps_ptr, stride_words, counts_ptr,
+                                        ctypes.byref(h)))
+        return PreparedBatch(self, h)
 
     def batch_config(self) -> dict:
         c = BatchConfig()

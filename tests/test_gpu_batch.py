@@ -158,3 +158,27 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
     check_batch(ctx, cols, qs)
     with pytest.raises(R.RtsError):
         ctx.set_batch_config(12, 256, 88 * 1024)
+
+
+def test_prepared_batch_graph_replays_match(ctx):
+    n = 333_333
+    cols = [D.uniform(n, 300), D.zipf(n, 301, 1.5), D.uniform(n, 302, 64)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 400, seed=21) + [[], [(2, 9, 3)], [(c, 1, 0xFFFFFF00) for c in range(3)]]
+    words = R.bitmap_words(n)
+    stride = (words + 31) // 32 * 32
+    out = torch.full((len(qs) * stride,), -1, dtype=torch.int32, device="cuda")
+    cnt = torch.full((len(qs),), -1, dtype=torch.int64, device="cuda")
+    pb = ctx.prepare_batch(qs, out.data_ptr(), stride, cnt.data_ptr())
+    s = torch.cuda.current_stream().cuda_stream
+    for rep in range(2):
+        out.fill_(-1)
+        cnt.fill_(-1)
+        pb.launch(s)
+        torch.cuda.synchronize()
+        o = out.cpu().numpy().view(np.uint32)
+        for i, q in enumerate(qs):
+            want, wcnt = expect(cols, q)
+            assert int(cnt[i].item()) == wcnt, (rep, i)
+            assert np.array_equal(o[i * stride:i * stride + words], want), (rep, i)
+    pb.release()
