@@ -383,11 +383,11 @@ def run(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded, generated on device)",
-        "config": {"workload": {"batched": f"batched scan 1e8 rows x 4 skewed columns, {nq} queries",
-                                "single": "single-column 1e8-row scan, 10% selectivity",
-                                "multi": "4-column 1e8-row conjunctive scan"}[wl],
+        "config": {"workload": {"batched": f"batched scan {n:.3g} rows x 4 skewed columns, {nq} queries",
+                                "single": f"single-column {n:.3g}-row scan, 10% selectivity",
+                                "multi": f"4-column {n:.3g}-row conjunctive scan"}[wl],
                    "nrows_per_gpu": n, "ncols": len(cols), "queries_per_step": nq,
-                   "column_kinds": kinds, "l2": "inputs larger than L2 (400 MB per column)"},
+                   "column_kinds": kinds, "l2": f"inputs larger than L2 ({n * 4 / 1e6:.0f} MB per column)"},
         "queries_per_s": round(nq * world / (ms_step * 1e-3), 1),
         "rows_per_s": round(n * world / (ms_step * 1e-3), 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
@@ -438,7 +438,7 @@ SERVE_KINDS = ["uniform", "uniform", "zipf1.3", "zipf1.3"]
 
 
 def served_leg(torch, R, D, ctx, dev, rank, args):
-    """Served scan (BASELINE config 5): a resident 2^28-row x 4-column table
+    """Served scan: a resident 2^28-row x 4-column table
     (2 uniform + 2 zipf 1.3 columns, 4 GiB), open-loop Poisson arrivals at
     several rates of queries over 1-4 columns with log-uniform selectivity,
     answered by the continuous-batching server; plus a burst of 256

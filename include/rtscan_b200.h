@@ -250,9 +250,12 @@ RTS_API void rts_batch_release(rts_prepared *p);
 
 /* ---- batched-kernel launch shape and its autotuner ------------------------ */
 typedef struct rts_batch_config {
-  int32_t warps_per_cta;        /* 8 or 16 (each warp stages 8 KiB of result words) */
-  int32_t max_queries_per_pass; /* 1..256 */
-  uint32_t table_budget_bytes;  /* shared memory a pass may use for its mask tables, 4..160 KiB */
+  int32_t variant;              /* 4: 512-query passes over 1024-row CTA blocks (default);
+                                   3: 256-query passes, one 256-row block per warp */
+  int32_t warps_per_cta;        /* variant 3: 8 or 16 (each warp stages 8 KiB of result words) */
+  int32_t max_queries_per_pass; /* 1..512 (variant 4), 1..256 (variant 3) */
+  uint32_t table_budget_bytes;  /* shared memory a pass may use for its mask tables: 4 KiB up to
+                                   136 KiB (variant 4), 88 KiB (variant 3, 16 warps), 140 KiB (8 warps) */
 } rts_batch_config;
 RTS_API rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg);
 RTS_API rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg);
@@ -275,7 +278,7 @@ RTS_API rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const
 typedef struct rts_server_config {
   int32_t max_active;         /* result slots (bitmap + count each); default 512 */
   int32_t max_queue;          /* requests waiting for a slot before RTS_ERR_FULL; default 65536 */
-  uint64_t segment_rows;      /* rows per scan step, a multiple of 256; default 2^22 */
+  uint64_t segment_rows;      /* rows per scan step, a multiple of 1024; default 2^22 */
   int32_t max_inflight_steps; /* steps queued on the GPU at once; default 2 */
 } rts_server_config;
 

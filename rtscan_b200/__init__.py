@@ -51,8 +51,8 @@ class ServerConfig(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     """rts_batch_config: launch shape of the batched kernel."""
-    _fields_ = [("warps_per_cta", ctypes.c_int32), ("max_queries_per_pass", ctypes.c_int32),
-                ("table_budget_bytes", ctypes.c_uint32)]
+    _fields_ = [("variant", ctypes.c_int32), ("warps_per_cta", ctypes.c_int32),
+                ("max_queries_per_pass", ctypes.c_int32), ("table_budget_bytes", ctypes.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -487,8 +487,9 @@ class Context:
         self._c(lib().rts_get_batch_config(self._h, ctypes.byref(c)))
         return c.as_dict()
 
-    def set_batch_config(self, warps_per_cta: int, max_queries_per_pass: int, table_budget_bytes: int):
-        c = BatchConfig(warps_per_cta, max_queries_per_pass, table_budget_bytes)
+    def set_batch_config(self, variant: int, warps_per_cta: int, max_queries_per_pass: int,
+                         table_budget_bytes: int):
+        c = BatchConfig(variant, warps_per_cta, max_queries_per_pass, table_budget_bytes)
         self._c(lib().rts_set_batch_config(self._h, ctypes.byref(c)))
 
     def autotune_batch(self, queries, cache_path: Optional[str] = None) -> dict:

@@ -31,6 +31,7 @@
 #include <cstring>
 #include <map>
 #include <set>
+#include <type_traits>
 #include <vector>
 
 #include "batch_plan.h"
@@ -53,7 +54,8 @@ struct BatchPass {
   uint32_t m[kMaxCols];         // boundaries of column c
   uint32_t bmin[kMaxCols];      // B[0]
   uint32_t bmax[kMaxCols];      // B[m-1]
-  uint32_t shift[kMaxCols];     // bucket = (x - bmin) >> shift
+  uint32_t shift[kMaxCols];     // linear buckets: bucket = (x - bmin) >> shift
+  uint32_t lgm[kMaxCols];       // > 0: log-linear buckets with lgm mantissa bits (bucket_of)
   uint32_t tab_off[kMaxCols];   // word offsets into the pass blob
   uint32_t bnd_off[kMaxCols];
   uint32_t bkt_off[kMaxCols];   // uint16 bucket starts, nbuckets+1 entries
@@ -66,17 +68,34 @@ struct BatchPass {
   unsigned long long *counts;
   uint64_t nrows;
   uint64_t words;               // bitmap words of one query
-  uint64_t block_begin;         // first 256-row block of the range
-  uint64_t nblocks;             // end of the range, in 256-row blocks
+  uint64_t block_begin;         // first block of the range (256 rows, 1024 for variant 4)
+  uint64_t nblocks;             // end of the range, in blocks
   int vec_store;                // bitmaps 16-byte aligned (out and stride)
 };
+
+// Log-linear bucket of v >= 0 with M mantissa bits: v itself below 2^M,
+// else 2^M buckets per octave, (e - M + 1) * 2^M + the M bits under the
+// leading one for v in [2^e, 2^(e+1)).  Monotone in v; at most
+// (33 - M) * 2^M buckets.  Skewed columns (a few dense small values and a
+// long tail) spread their boundaries over these buckets far more evenly
+// than over linear ones.
+__host__ __device__ __forceinline__ uint32_t bucket_of(uint32_t v, uint32_t M) {
+#ifdef __CUDA_ARCH__
+  const int e = 31 - __clz(v);  // -1 for v = 0
+#else
+  const int e = v ? 31 - __builtin_clz(v) : -1;
+#endif
+  const uint32_t sh = e > (int)M ? (uint32_t)(e - (int)M) : 0u;
+  return (sh << M) + (v >> sh);
+}
 
 // Position of x among the boundaries of column c: #{B[i] <= x}.
 __device__ __forceinline__ uint32_t position(const BatchPass &p, const uint32_t *sm, int c, uint32_t x) {
   const uint32_t m = p.m[c];
   if (m == 0 || x < p.bmin[c]) return 0;
   if (x >= p.bmax[c]) return m;
-  const uint32_t k = (x - p.bmin[c]) >> p.shift[c];
+  const uint32_t v = x - p.bmin[c];
+  const uint32_t k = p.lgm[c] ? bucket_of(v, p.lgm[c]) : v >> p.shift[c];
   const uint16_t *bk = reinterpret_cast<const uint16_t *>(sm + p.bkt_off[c]);
   uint32_t lo = bk[k], hi = bk[k + 1];  // boundaries of bucket k: B[lo..hi)
   const uint32_t *B = sm + p.bnd_off[c];
@@ -309,6 +328,26 @@ void launch_one(const BatchPass &bp, int sm_count, cudaStream_t s) {
   batch_kernel<CMAX, W><<<grid, W * 32, sm, s>>>(bp);
 }
 
+#include "batch4.cuh"
+
+template <int CMAX>
+size_t smem_bytes4(uint32_t blob_words) {
+  return ((blob_words + 3) & ~3u) * 4 + (size_t)kV4StageWords * 4 + (size_t)kV4PosBytes<CMAX>;
+}
+
+template <int CMAX>
+void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(batch4_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    attr_set = true;
+  }
+  const size_t sm = smem_bytes4<CMAX>(bp.blob_words);
+  const uint64_t want = bp.nblocks - bp.block_begin;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count));
+  batch4_kernel<CMAX><<<grid, kV4Threads, sm, s>>>(bp);
+}
+
 }  // namespace
 
 // ---- host planning -----------------------------------------------------------
@@ -353,26 +392,26 @@ struct PassPlan {
 
 // Shared-memory bytes of a pass's tables, boundaries and bucket index for
 // the given boundary counts (bucket index at most 4097 uint16 per column).
-size_t column_bytes(size_t m) {
+size_t column_bytes(size_t m, int G) {
   size_t nb = 1;
   while (nb < 4 * m && nb < 4096) nb <<= 1;
-  return (m + 1) * kGroups * 4 + m * 4 + (nb + 2) * 2 + 8;
+  return (m + 1) * (size_t)G * 4 + m * 4 + (nb + 2) * 2 + 8;
 }
 
-// Add query q to the pass if its tables still fit the budget.
-bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_per_pass) {
-  if ((int)pp.qs.size() >= std::min(max_per_pass, kSlots)) return false;
+// Add query q to the pass if its tables still fit the budget (G words of
+// 32 query bits per table row).
+bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_per_pass, int G) {
+  if ((int)pp.qs.size() >= std::min(max_per_pass, 32 * G)) return false;
   size_t total = 0;
   int new_cols = 0;
   std::vector<size_t> grow(pp.cols.size(), 0);
-  std::vector<uint32_t> extra_new;  // boundaries of columns new to the pass
   for (size_t k = 0; k < q.cols.size(); k++) {
     auto it = std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]);
     size_t add = 0;
     if (it == pp.cols.end()) {
       new_cols++;
       add = (q.lo[k] > 0) + (q.hi[k] < 0xFFFFFFFFu);
-      total += column_bytes(add);
+      total += column_bytes(add, G);
     } else {
       const auto &S = pp.bounds[it - pp.cols.begin()];
       if (q.lo[k] > 0 && !S.count(q.lo[k])) grow[it - pp.cols.begin()]++;
@@ -380,7 +419,7 @@ bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_pe
     }
   }
   if ((int)pp.cols.size() + new_cols > kMaxCols) return false;
-  for (size_t c = 0; c < pp.cols.size(); c++) total += column_bytes(pp.bounds[c].size() + grow[c]);
+  for (size_t c = 0; c < pp.cols.size(); c++) total += column_bytes(pp.bounds[c].size() + grow[c], G);
   if (total > budget && !pp.qs.empty()) return false;
   for (size_t k = 0; k < q.cols.size(); k++) {
     auto it = std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]);
@@ -432,6 +471,7 @@ struct BatchPlan {
     BatchPass bp;
     size_t off;  // word offset of the pass in `blob`
     int cmax;
+    int variant;  // kernel the pass was planned for (3: 8 groups, 4: 16 groups)
   };
   std::vector<Pass> passes;
   std::vector<uint32_t> blob;
@@ -477,18 +517,71 @@ int launch_outside(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::
   return launches;
 }
 
+// Bucket index of a pass column's sorted boundaries B (B[0] = bmin, values
+// up to bmin + span - 1): entry k is the first boundary in bucket k, so a
+// value in bucket k only needs a search among B[bk[k] .. bk[k+1]).  Both the
+// linear mapping (shift) and the log-linear one (bucket_of, mantissa bits
+// *lgm) are built with at most nb_target buckets, and the one with the
+// smaller mean search depth over the boundary intervals is kept (queries
+// place their bounds at value quantiles, so each interval stands for about
+// the same share of rows).  *lgm = 0 selects the linear mapping.
+std::vector<uint16_t> bucket_index(const std::vector<uint32_t> &B, uint64_t span, uint32_t nb_target,
+                                   uint32_t *shift_out, uint32_t *lgm_out) {
+  const uint32_t m = (uint32_t)B.size(), bmin = B.front();
+  auto depth = [&](const std::vector<uint16_t> &bk, auto &&bucket) {
+    double d = 0;
+    for (uint32_t i = 0; i + 1 < m; i++) {
+      const uint32_t k = bucket(B[i] - bmin);
+      uint32_t n = (uint32_t)(bk[k + 1] - bk[k]), it = 0;
+      while (n) { it++; n >>= 1; }
+      d += it;
+    }
+    return d;
+  };
+  uint32_t shift = 0;
+  while ((span >> shift) > nb_target) shift++;
+  const uint32_t nb = (uint32_t)(((span - 1) >> shift) + 1);  // buckets covering [bmin, bmax]
+  std::vector<uint16_t> lin(nb + 1);
+  for (uint32_t k = 0; k <= nb; k++) {
+    const uint64_t start = (uint64_t)bmin + ((uint64_t)k << shift);
+    lin[k] = start > 0xFFFFFFFFull ? (uint16_t)m
+                                    : (uint16_t)(std::lower_bound(B.begin(), B.end(), (uint32_t)start) - B.begin());
+  }
+  *shift_out = shift;
+  *lgm_out = 0;
+  uint32_t M = 12;
+  while (M > 0 && bucket_of((uint32_t)(span - 1), M) + 1 > nb_target) M--;
+  if (M == 0) return lin;
+  const uint32_t nbl = bucket_of((uint32_t)(span - 1), M) + 1;
+  std::vector<uint16_t> lg(nbl + 1, 0);
+  uint32_t i = 0;
+  for (uint32_t k = 0; k <= nbl; k++) {  // first boundary whose bucket is >= k
+    while (i < m && bucket_of(B[i] - bmin, M) < k) i++;
+    lg[k] = (uint16_t)i;
+  }
+  const double dl = depth(lin, [&](uint32_t v) { return v >> shift; });
+  const double dg = depth(lg, [&](uint32_t v) { return bucket_of(v, M); });
+  if (dg < dl) {
+    *lgm_out = M;
+    return lg;
+  }
+  return lin;
+}
+
 bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && (int)q.cols.size() <= kMaxCols; }
 
 // Passes for the kernel queries `which` (indices into norm); query qi writes
 // bitmap out_index[qi] (qi when null).
 BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
                      const int32_t *out_index, size_t table_budget) {
+  const int variant = ctx->batch_cfg.variant == 4 ? 4 : 3;
+  const int G = variant == 4 ? kV4Groups : kGroups;  // table words per position
   std::vector<PassPlan> passes;
   for (int qi : which) {
     const int per = ctx->batch_cfg.max_queries_per_pass;
-    if (passes.empty() || !try_add(passes.back(), norm[qi], qi, table_budget, per)) {
+    if (passes.empty() || !try_add(passes.back(), norm[qi], qi, table_budget, per, G)) {
       passes.emplace_back();
-      if (!try_add(passes.back(), norm[qi], qi, table_budget, per))
+      if (!try_add(passes.back(), norm[qi], qi, table_budget, per, G))
         throw Error(RTS_ERR_ARG, "query does not fit one batch pass");
     }
   }
@@ -510,8 +603,8 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       const uint32_t m = (uint32_t)B[c].size();
       bp.m[c] = m;
       bp.tab_off[c] = (uint32_t)blob.size();
-      blob.resize(blob.size() + (size_t)(m + 1) * kGroups, 0u);
-      std::vector<uint32_t> delta((size_t)(m + 2) * kGroups, 0u);
+      blob.resize(blob.size() + (size_t)(m + 1) * G, 0u);
+      std::vector<uint32_t> delta((size_t)(m + 2) * G, 0u);
       auto pos_of = [&](uint32_t x) {  // #boundaries <= x
         return (uint32_t)(std::upper_bound(B[c].begin(), B[c].end(), x) - B[c].begin());
       };
@@ -526,15 +619,15 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
           p0 = pos_of(q.lo[k]);
           p1 = pos_of(q.hi[k]);
         }
-        delta[(size_t)p0 * kGroups + grp] ^= bit;
-        delta[(size_t)(p1 + 1) * kGroups + grp] ^= bit;
+        delta[(size_t)p0 * G + grp] ^= bit;
+        delta[(size_t)(p1 + 1) * G + grp] ^= bit;
       }
       uint32_t *tab = blob.data() + bp.tab_off[c];
-      for (int grp = 0; grp < kGroups; grp++) {
+      for (int grp = 0; grp < G; grp++) {
         uint32_t acc = 0;
         for (uint32_t pos = 0; pos <= m; pos++) {
-          acc ^= delta[(size_t)pos * kGroups + grp];
-          tab[(size_t)pos * kGroups + grp] = acc;
+          acc ^= delta[(size_t)pos * G + grp];
+          tab[(size_t)pos * G + grp] = acc;
         }
       }
     }
@@ -553,23 +646,14 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       const uint64_t span = (uint64_t)bp.bmax[c] - bp.bmin[c] + 1;
       uint32_t nb_target = 1;
       while (nb_target < 4 * m && nb_target < 4096) nb_target <<= 1;
-      uint32_t shift = 0;
-      while ((span >> shift) > nb_target) shift++;
-      bp.shift[c] = shift;
-      const uint32_t nb = (uint32_t)(((span - 1) >> shift) + 1);  // buckets covering [bmin, bmax]
-      std::vector<uint16_t> bk(nb + 1);
-      for (uint32_t k = 0; k <= nb; k++) {
-        const uint64_t start = (uint64_t)bp.bmin[c] + ((uint64_t)k << shift);
-        bk[k] = (uint16_t)(std::lower_bound(B[c].begin(), B[c].end(), start) - B[c].begin());
-        if (start > 0xFFFFFFFFull) bk[k] = (uint16_t)m;
-      }
+      const std::vector<uint16_t> bk = bucket_index(B[c], span, nb_target, &bp.shift[c], &bp.lgm[c]);
       bp.bkt_off[c] = (uint32_t)blob.size();
       const size_t wsz = (bk.size() + 1) / 2;
       blob.resize(blob.size() + wsz, 0u);
       memcpy(blob.data() + bp.bkt_off[c], bk.data(), bk.size() * 2);
     }
     bp.slot_off = (uint32_t)blob.size();
-    for (int slot = 0; slot < kSlots; slot++) {
+    for (int slot = 0; slot < 32 * G; slot++) {
       uint32_t o = 0xFFFFFFFFu;
       if (slot < (int)pp.qs.size()) o = out_index ? (uint32_t)out_index[pp.qs[slot]] : (uint32_t)pp.qs[slot];
       blob.push_back(o);
@@ -577,6 +661,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     bp.blob_words = (uint32_t)blob.size();
     for (int c = 0; c < C; c++) bp.col[c] = ctx->cols[pp.cols[c]];
     b.cmax = C <= 4 ? 4 : 8;
+    b.variant = variant;
     while (plan.blob.size() % 4) plan.blob.push_back(0);  // 16-byte aligned pass start
     b.off = plan.blob.size();
     plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
@@ -586,12 +671,13 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
 }
 
 // Launch every pass of `plan` (blob already on the device) over rows
-// [row_begin, row_end); row_begin is a multiple of 256.  Returns launches.
+// [row_begin, row_end); row_begin is a multiple of 1024 (the larger block of
+// the two kernel variants).  Returns launches.
 int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
                 unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
-  const uint64_t rows_per_block = 32 * kTilesPerBlock;
   int launches = 0;
   for (auto &b : plan.passes) {
+    const uint64_t rows_per_block = b.variant == 4 ? (uint64_t)kV4Rows : (uint64_t)(32 * kTilesPerBlock);
     BatchPass bp = b.bp;
     bp.blob = dev_blob + b.off;
     bp.out = out;
@@ -603,7 +689,10 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.nblocks = (row_end + rows_per_block - 1) / rows_per_block;
     bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
-    if (b.cmax == 4) {
+    if (b.variant == 4) {
+      if (b.cmax == 4) launch_one4<4>(bp, ctx->sm_count, s);
+      else launch_one4<8>(bp, ctx->sm_count, s);
+    } else if (b.cmax == 4) {
       if (w8) launch_one<4, 8>(bp, ctx->sm_count, s);
       else launch_one<4, 16>(bp, ctx->sm_count, s);
     } else {

@@ -104,9 +104,10 @@ void destroy_host_batch(HostBatchBuffers *b);
 // pass (<= 256) and the shared-memory bytes a pass may spend on its mask
 // tables (the rest of the CTA's shared memory stages result words).
 struct BatchConfig {
-  int warps_per_cta = 16;
-  int max_queries_per_pass = 256;
-  size_t table_budget = 88 * 1024;
+  int variant = 4;                // 4: 512-query passes, CTA-wide 1024-row blocks; 3: 256-query passes per warp
+  int warps_per_cta = 16;         // variant 3 only
+  int max_queries_per_pass = 512;
+  size_t table_budget = 136 * 1024;
 };
 void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq, uint32_t *out,
                 uint64_t stride_words, unsigned long long *counts, cudaStream_t s, size_t table_budget);

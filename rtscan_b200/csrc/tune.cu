@@ -22,14 +22,19 @@
 namespace {
 
 struct Candidate {
-  int warps, qpp;
+  int variant, warps, qpp;
   size_t budget;
 };
 
 const Candidate kCandidates[] = {
-    {16, 256, 88 * 1024}, {16, 256, 64 * 1024}, {16, 128, 88 * 1024},
-    {8, 256, 40 * 1024},  {8, 128, 40 * 1024},  {8, 256, 140 * 1024},
+    {4, 16, 512, 136 * 1024}, {4, 16, 384, 136 * 1024}, {4, 16, 256, 96 * 1024},
+    {3, 16, 256, 88 * 1024},  {3, 16, 256, 64 * 1024},  {3, 8, 256, 40 * 1024}, {3, 8, 256, 140 * 1024},
 };
+
+size_t max_budget(int variant, int warps) {
+  if (variant == 4) return 136 * 1024;
+  return warps == 16 ? 88 * 1024 : 140 * 1024;
+}
 
 std::string cache_key(rts_ctx *ctx, int nq) {
   cudaDeviceProp p;
@@ -53,10 +58,11 @@ bool cache_lookup(const char *path, const std::string &key, rts::BatchConfig *ou
   bool found = false;
   while (fgets(line, sizeof line, f)) {
     char k[400];
-    int w, q;
+    int v, w, q;
     unsigned long b;
     double ms;
-    if (sscanf(line, "%399s %d %d %lu %lf", k, &w, &q, &b, &ms) == 5 && key == k) {
+    if (sscanf(line, "%399s %d %d %d %lu %lf", k, &v, &w, &q, &b, &ms) == 6 && key == k) {
+      out->variant = v;
       out->warps_per_cta = w;
       out->max_queries_per_pass = q;
       out->table_budget = b;
@@ -71,14 +77,17 @@ void cache_store(const char *path, const std::string &key, const rts::BatchConfi
   if (!path) return;
   FILE *f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%s %d %d %lu %.4f\n", key.c_str(), c.warps_per_cta, c.max_queries_per_pass,
+  fprintf(f, "%s %d %d %d %lu %.4f\n", key.c_str(), c.variant, c.warps_per_cta, c.max_queries_per_pass,
           (unsigned long)c.table_budget, ms);
   fclose(f);
 }
 
 bool valid(const rts_batch_config &c) {
-  return (c.warps_per_cta == 8 || c.warps_per_cta == 16) && c.max_queries_per_pass >= 1 &&
-         c.max_queries_per_pass <= 256 && c.table_budget_bytes >= 4096 && c.table_budget_bytes <= 160 * 1024;
+  if (c.variant != 3 && c.variant != 4) return false;
+  if (c.warps_per_cta != 8 && c.warps_per_cta != 16) return false;
+  const int max_q = c.variant == 4 ? 512 : 256;
+  return c.max_queries_per_pass >= 1 && c.max_queries_per_pass <= max_q && c.table_budget_bytes >= 4096 &&
+         c.table_budget_bytes <= max_budget(c.variant, c.warps_per_cta);
 }
 
 }  // namespace
@@ -88,9 +97,11 @@ extern "C" {
 rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg) {
   if (!ctx || !cfg) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
   if (!valid(*cfg)) {
-    ctx->err = "batch config out of range (warps 8|16, 1..256 queries per pass, 4..160 KiB table budget)";
+    ctx->err = "batch config out of range (variant 3|4, warps 8|16, queries per pass and table budget within "
+               "the variant's limits)";
     return rts::set_thread_error(RTS_ERR_ARG, ctx->err);
   }
+  ctx->batch_cfg.variant = cfg->variant;
   ctx->batch_cfg.warps_per_cta = cfg->warps_per_cta;
   ctx->batch_cfg.max_queries_per_pass = cfg->max_queries_per_pass;
   ctx->batch_cfg.table_budget = cfg->table_budget_bytes;
@@ -99,6 +110,7 @@ rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg) {
 
 rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg) {
   if (!ctx || !cfg) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
+  cfg->variant = ctx->batch_cfg.variant;
   cfg->warps_per_cta = ctx->batch_cfg.warps_per_cta;
   cfg->max_queries_per_pass = ctx->batch_cfg.max_queries_per_pass;
   cfg->table_budget_bytes = (uint32_t)ctx->batch_cfg.table_budget;
@@ -140,6 +152,7 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
     double best_ms = 1e300;
     rts::BatchConfig best = saved_cfg;
     for (const Candidate &c : kCandidates) {
+      ctx->batch_cfg.variant = c.variant;
       ctx->batch_cfg.warps_per_cta = c.warps;
       ctx->batch_cfg.max_queries_per_pass = c.qpp;
       ctx->batch_cfg.table_budget = c.budget;

@@ -92,6 +92,33 @@ def test_batch_many_columns_per_pass(ctx):
     check_batch(ctx, cols, qs)
 
 
+def test_batch_skewed_boundaries(ctx):
+    """Bounds packed into small values plus powers of two up to 2^32 - 1 (the
+    shape for which the planner indexes boundaries by log-linear buckets),
+    with rows sitting on and next to every bound."""
+    n = 120_000
+    rng = np.random.default_rng(5)
+    edges = [0, 1, 2] + [v for k in range(2, 33) for v in ((1 << k) - 2, (1 << k) - 1, 1 << k)
+                         if v <= 0xFFFFFFFF]
+    edges = np.array(sorted(set(e for e in edges if e <= 0xFFFFFFFF)), dtype=np.uint64)
+    near = rng.choice(edges, size=n // 2)
+    small = rng.integers(0, 400, size=n // 4)
+    wide = rng.integers(0, 1 << 32, size=n - n // 2 - n // 4)
+    col = np.concatenate([near, small, wide]).astype(np.uint32)
+    rng.shuffle(col)
+    cols = [col, D.zipf(n, 7, 1.5)]
+    ctx.load_columns(cols)
+    pool = [int(e) for e in edges] + list(range(0, 400, 3))
+    qs = []
+    for i in range(500):
+        a, b = sorted(int(x) for x in rng.choice(pool, size=2))
+        q = [(0, a, b)]
+        if i % 3 == 0:
+            q.append((1, int(rng.integers(0, 20)), int(rng.integers(20, 3000))))
+        qs.append(q)
+    check_batch(ctx, cols, qs)
+
+
 def test_batch_duplicate_heavy(ctx):
     n = 200_000
     cols = [D.uniform(n, 80, 2), D.uniform(n, 81, 64), D.zipf(n, 82, 1.5)]
@@ -129,8 +156,9 @@ def test_batch_alone_and_in_the_mix(ctx):
         assert np.array_equal(alone[0], mixed[i][0])
 
 
-@pytest.mark.parametrize("cfg", [(16, 256, 88 * 1024), (16, 64, 16 * 1024), (8, 256, 40 * 1024),
-                                 (8, 128, 140 * 1024), (8, 1, 4096)])
+@pytest.mark.parametrize("cfg", [(4, 16, 512, 136 * 1024), (4, 16, 100, 136 * 1024), (4, 16, 512, 8 * 1024),
+                                 (3, 16, 256, 88 * 1024), (3, 16, 64, 16 * 1024), (3, 8, 256, 40 * 1024),
+                                 (3, 8, 128, 140 * 1024), (3, 8, 1, 4096), (4, 16, 1, 4096)])
 def test_batch_every_launch_shape(ctx, cfg):
     n = 150_011
     cols = [D.uniform(n, 200), D.zipf(n, 201, 1.1), D.uniform(n, 202, 1000), D.normal(n, 203)]
@@ -138,9 +166,10 @@ def test_batch_every_launch_shape(ctx, cfg):
     old = ctx.batch_config()
     ctx.set_batch_config(*cfg)
     try:
-        check_batch(ctx, cols, D.batch_queries(cols, 300, seed=cfg[1]))
+        check_batch(ctx, cols, D.batch_queries(cols, 600, seed=cfg[2]) + [[], [(1, 3, 2)]])
     finally:
-        ctx.set_batch_config(old["warps_per_cta"], old["max_queries_per_pass"], old["table_budget_bytes"])
+        ctx.set_batch_config(old["variant"], old["warps_per_cta"], old["max_queries_per_pass"],
+                             old["table_budget_bytes"])
 
 
 def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
@@ -150,14 +179,16 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
     qs = D.batch_queries(cols, 200, seed=4)
     cache = str(tmp_path / "tune.txt")
     best = ctx.autotune_batch(qs, cache)
-    assert best["warps_per_cta"] in (8, 16)
-    assert 1 <= best["max_queries_per_pass"] <= 256
+    assert best["variant"] in (3, 4) and best["warps_per_cta"] in (8, 16)
+    assert 1 <= best["max_queries_per_pass"] <= 512
     assert open(cache).read().strip()
     again = ctx.autotune_batch(qs, cache)  # served from the cache
     assert again == best
     check_batch(ctx, cols, qs)
     with pytest.raises(R.RtsError):
-        ctx.set_batch_config(12, 256, 88 * 1024)
+        ctx.set_batch_config(3, 12, 256, 88 * 1024)
+    with pytest.raises(R.RtsError):
+        ctx.set_batch_config(4, 16, 513, 88 * 1024)
 
 
 def test_prepared_batch_graph_replays_match(ctx):
