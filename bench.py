@@ -51,6 +51,32 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+# DRAM traffic of the dominant kernel from one ncu capture each
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) beside that
+# launch's own bytes: columns read once and one bitmap written per query of
+# the launch.  A launch of the timed workload is credited with the same
+# traffic-to-bytes ratio (the kernel streams each column once per launch and
+# writes each bitmap once, so its traffic grows in proportion).
+NCU_TRAFFIC = {
+    "batched": {"kernel": "batch4_kernel<4>", "capture": "3e7 rows x 4 columns, 512 queries, one launch",
+                "bytes": 480.2e6 + 1862.6e6, "launch_bytes": 4 * 4 * 3e7 + 512 * 3e7 / 8},
+    "single": {"kernel": "scan_fused_kernel<1,1>", "capture": "1e8 rows x 1 column, one launch",
+               "bytes": 408.9e6, "launch_bytes": 4 * 1e8 + 1e8 / 8},
+}
+
+
+def launch_traffic(wl, n, queries, launches):
+    """Traffic of one launch of the timed workload scaled from its capture."""
+    cap = NCU_TRAFFIC.get(wl)
+    if cap is None:
+        return None
+    used = {c for q in queries for c, _, _ in q}
+    own = 4 * n * len(used) + (len(queries) / launches) * n / 8
+    return {"bytes": round(cap["bytes"] / cap["launch_bytes"] * own / 1e9, 3), "unit": "GB",
+            "kernel": cap["kernel"], "capture": cap["capture"],
+            "launch_bytes_GB": round(own / 1e9, 3)}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -304,6 +330,7 @@ def run(args):
     kern_launches = max(1, launches // args.steps)
     ms_launch = statistics.median(per) / kern_launches
     achieved = (bytes_step / kern_launches) / (ms_launch * 1e-3) / 1e9
+    tr = launch_traffic(wl, n, queries, kern_launches)
 
     extra = {}
     if wl == "multi":
@@ -391,7 +418,8 @@ def run(args):
         "queries_per_s": round(nq * world / (ms_step * 1e-3), 1),
         "rows_per_s": round(n * world / (ms_step * 1e-3), 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                     "frac": round(achieved / hbm_peak, 4),
+                     "traffic": (tr or {}).get("bytes"), "traffic_unit": "GB per launch", "traffic_detail": tr,
                      "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel_launches_per_step": kern_launches},
         "e2e": e2e,
