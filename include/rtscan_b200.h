@@ -278,7 +278,7 @@ RTS_API rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const
 typedef struct rts_server_config {
   int32_t max_active;         /* result slots (bitmap + count each); default 512 */
   int32_t max_queue;          /* requests waiting for a slot before RTS_ERR_FULL; default 65536 */
-  uint64_t segment_rows;      /* rows per scan step, a multiple of 1024; default 2^22 */
+  uint64_t segment_rows;      /* rows per scan step, a multiple of 4096; default 2^22 */
   int32_t max_inflight_steps; /* steps queued on the GPU at once; default 2 */
 } rts_server_config;
 

@@ -58,7 +58,8 @@ struct BatchPass {
   uint32_t lgm[kMaxCols];       // > 0: log-linear buckets with lgm mantissa bits (bucket_of)
   uint32_t tab_off[kMaxCols];   // word offsets into the pass blob
   uint32_t bnd_off[kMaxCols];
-  uint32_t bkt_off[kMaxCols];   // uint16 bucket starts, nbuckets+1 entries
+  uint32_t bkt_off[kMaxCols];   // uint16 bucket starts, nbk+1 entries
+  uint32_t nbk[kMaxCols];       // buckets of column c
   int ncols;
   uint32_t blob_words;          // words of the blob copied to shared memory
   const uint32_t *blob;         // tables | boundaries | buckets | slot map (global)
@@ -87,6 +88,26 @@ __host__ __device__ __forceinline__ uint32_t bucket_of(uint32_t v, uint32_t M) {
 #endif
   const uint32_t sh = e > (int)M ? (uint32_t)(e - (int)M) : 0u;
   return (sh << M) + (v >> sh);
+}
+
+// Position of x among the boundaries of column c from the bucket index
+// alone, without a loop: exact (and *exact set) when x's bucket holds at
+// most two boundaries, the usual case; callers redo the others with
+// position().  Every load stays inside the pass blob: a value below B[0]
+// or above the last bucket is clamped to a bucket, and B[lo + 1] past the
+// boundaries reads the bucket index that follows them.
+__device__ __forceinline__ uint32_t position_fast(const BatchPass &p, const uint32_t *sm, int c, uint32_t x,
+                                                  bool &exact) {
+  const uint32_t v = x - p.bmin[c];
+  const uint32_t k = min(p.lgm[c] ? bucket_of(v, p.lgm[c]) : v >> p.shift[c], p.nbk[c] - 1);
+  const uint16_t *bk = reinterpret_cast<const uint16_t *>(sm + p.bkt_off[c]);
+  const uint32_t lo = bk[k], hi = bk[k + 1];
+  const uint32_t *B = sm + p.bnd_off[c];
+  const uint32_t b0 = B[lo], b1 = B[lo + 1];
+  const bool below = x < p.bmin[c];
+  exact = below || hi - lo <= 2;
+  const uint32_t pos = lo + (hi > lo && b0 <= x) + (hi > lo + 1 && b1 <= x);
+  return below ? 0u : pos;
 }
 
 // Position of x among the boundaries of column c: #{B[i] <= x}.
@@ -329,23 +350,25 @@ void launch_one(const BatchPass &bp, int sm_count, cudaStream_t s) {
 }
 
 #include "batch4.cuh"
+#include "batch_few.cuh"
 
-template <int CMAX>
+template <int CMAX, int GV>
 size_t smem_bytes4(uint32_t blob_words) {
-  return ((blob_words + 3) & ~3u) * 4 + (size_t)kV4StageWords * 4 + (size_t)kV4PosBytes<CMAX>;
+  return ((blob_words + 3) & ~3u) * 4 + (size_t)kV4StageWords * 4 + (size_t)kV4PosBytes<CMAX, GV>;
 }
 
-template <int CMAX>
+template <int CMAX, int GV>
 void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(batch4_kernel<CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(batch4_kernel<CMAX, GV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     attr_set = true;
   }
-  const size_t sm = smem_bytes4<CMAX>(bp.blob_words);
+  const size_t sm = smem_bytes4<CMAX, GV>(bp.blob_words);
+  if (sm > 227 * 1024) throw Error(RTS_ERR_ARG, "batch pass exceeds shared memory");
   const uint64_t want = bp.nblocks - bp.block_begin;
   const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count));
-  batch4_kernel<CMAX><<<grid, kV4Threads, sm, s>>>(bp);
+  batch4_kernel<CMAX, GV><<<grid, kV4Threads, sm, s>>>(bp);
 }
 
 }  // namespace
@@ -471,7 +494,10 @@ struct BatchPlan {
     BatchPass bp;
     size_t off;  // word offset of the pass in `blob`
     int cmax;
-    int variant;  // kernel the pass was planned for (3: 8 groups, 4: 16 groups)
+    int variant;  // kernel the pass was planned for (3: 256-slot warps, 4: CTA-wide blocks)
+    int groups;   // 32-slot groups of the pass (table words per position)
+    bool few;     // at most 32 queries: tested term by term (batch_few_kernel), no tables
+    FewPass fp;
   };
   std::vector<Pass> passes;
   std::vector<uint32_t> blob;
@@ -570,12 +596,15 @@ std::vector<uint16_t> bucket_index(const std::vector<uint32_t> &B, uint64_t span
 
 bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && (int)q.cols.size() <= kMaxCols; }
 
+// Slot groups of a variant-4 pass of nq queries.
+int pass_groups(int nq) { return nq <= 128 ? 4 : nq <= 256 ? 8 : 16; }
+
 // Passes for the kernel queries `which` (indices into norm); query qi writes
 // bitmap out_index[qi] (qi when null).
 BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
                      const int32_t *out_index, size_t table_budget) {
   const int variant = ctx->batch_cfg.variant == 4 ? 4 : 3;
-  const int G = variant == 4 ? kV4Groups : kGroups;  // table words per position
+  const int G = variant == 4 ? 16 : kGroups;  // pass capacity in groups (budgeted at this table width)
   std::vector<PassPlan> passes;
   for (int qi : which) {
     const int per = ctx->batch_cfg.max_queries_per_pass;
@@ -589,8 +618,36 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
   for (auto &pp : passes) {
     BatchPlan::Pass b;
     memset(&b.bp, 0, sizeof b.bp);
-    BatchPass &bp = b.bp;
+    memset(&b.fp, 0, sizeof b.fp);
+    b.few = false;
     const int C = (int)pp.cols.size();
+    if (variant == 4 && (int)pp.qs.size() <= kFewSlots) {
+      FewPass &fp = b.fp;
+      b.few = true;
+      b.variant = variant;
+      b.groups = 1;
+      b.cmax = C <= 4 ? 4 : 8;
+      fp.nq = (int)pp.qs.size();
+      fp.ncols = C;
+      for (int c = 0; c < C; c++) fp.col[c] = ctx->cols[pp.cols[c]];
+      for (int j = 0; j < kFewSlots; j++) fp.slot_query[j] = -1;
+      for (int j = 0; j < fp.nq; j++) {
+        const NormQuery &q = norm[pp.qs[j]];
+        fp.slot_query[j] = out_index ? out_index[pp.qs[j]] : pp.qs[j];
+        for (size_t k = 0; k < q.cols.size(); k++) {
+          const int c = (int)(std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]) - pp.cols.begin());
+          fp.colmask[j] |= 1u << c;
+          fp.term[j][c] = make_uint2(q.lo[k], q.hi[k] - q.lo[k]);
+        }
+      }
+      b.off = plan.blob.size();
+      plan.passes.push_back(b);
+      continue;
+    }
+    BatchPass &bp = b.bp;
+    // 4: the smallest of the 128-, 256- and 512-slot shapes that holds the pass
+    const int Gp = variant == 4 ? pass_groups((int)pp.qs.size()) : kGroups;
+    b.groups = Gp;
     bp.ncols = C;
     std::vector<uint32_t> blob;
     std::vector<std::vector<uint32_t>> B(C);
@@ -603,8 +660,8 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       const uint32_t m = (uint32_t)B[c].size();
       bp.m[c] = m;
       bp.tab_off[c] = (uint32_t)blob.size();
-      blob.resize(blob.size() + (size_t)(m + 1) * G, 0u);
-      std::vector<uint32_t> delta((size_t)(m + 2) * G, 0u);
+      blob.resize(blob.size() + (size_t)(m + 1) * Gp, 0u);
+      std::vector<uint32_t> delta((size_t)(m + 2) * Gp, 0u);
       auto pos_of = [&](uint32_t x) {  // #boundaries <= x
         return (uint32_t)(std::upper_bound(B[c].begin(), B[c].end(), x) - B[c].begin());
       };
@@ -619,15 +676,15 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
           p0 = pos_of(q.lo[k]);
           p1 = pos_of(q.hi[k]);
         }
-        delta[(size_t)p0 * G + grp] ^= bit;
-        delta[(size_t)(p1 + 1) * G + grp] ^= bit;
+        delta[(size_t)p0 * Gp + grp] ^= bit;
+        delta[(size_t)(p1 + 1) * Gp + grp] ^= bit;
       }
       uint32_t *tab = blob.data() + bp.tab_off[c];
-      for (int grp = 0; grp < G; grp++) {
+      for (int grp = 0; grp < Gp; grp++) {
         uint32_t acc = 0;
         for (uint32_t pos = 0; pos <= m; pos++) {
-          acc ^= delta[(size_t)pos * G + grp];
-          tab[(size_t)pos * G + grp] = acc;
+          acc ^= delta[(size_t)pos * Gp + grp];
+          tab[(size_t)pos * Gp + grp] = acc;
         }
       }
     }
@@ -638,6 +695,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       blob.insert(blob.end(), B[c].begin(), B[c].end());
       if (m == 0) {
         bp.bkt_off[c] = (uint32_t)blob.size();
+        bp.nbk[c] = 1;
         blob.push_back(0);
         continue;
       }
@@ -647,13 +705,14 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       uint32_t nb_target = 1;
       while (nb_target < 4 * m && nb_target < 4096) nb_target <<= 1;
       const std::vector<uint16_t> bk = bucket_index(B[c], span, nb_target, &bp.shift[c], &bp.lgm[c]);
+      bp.nbk[c] = (uint32_t)bk.size() - 1;
       bp.bkt_off[c] = (uint32_t)blob.size();
       const size_t wsz = (bk.size() + 1) / 2;
       blob.resize(blob.size() + wsz, 0u);
       memcpy(blob.data() + bp.bkt_off[c], bk.data(), bk.size() * 2);
     }
     bp.slot_off = (uint32_t)blob.size();
-    for (int slot = 0; slot < 32 * G; slot++) {
+    for (int slot = 0; slot < 32 * Gp; slot++) {
       uint32_t o = 0xFFFFFFFFu;
       if (slot < (int)pp.qs.size()) o = out_index ? (uint32_t)out_index[pp.qs[slot]] : (uint32_t)pp.qs[slot];
       blob.push_back(o);
@@ -671,13 +730,40 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
 }
 
 // Launch every pass of `plan` (blob already on the device) over rows
-// [row_begin, row_end); row_begin is a multiple of 1024 (the larger block of
-// the two kernel variants).  Returns launches.
+// [row_begin, row_end); row_begin is a multiple of 4096 (the largest block
+// of the pass shapes).  Returns launches.
 int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
                 unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
   int launches = 0;
   for (auto &b : plan.passes) {
-    const uint64_t rows_per_block = b.variant == 4 ? (uint64_t)kV4Rows : (uint64_t)(32 * kTilesPerBlock);
+    if (b.few) {
+      FewPass fp = b.fp;
+      fp.out = out;
+      fp.stride_words = stride_words;
+      fp.counts = counts;
+      fp.nrows = row_end;
+      fp.words = words_for(ctx->nrows);
+      fp.tile_begin = row_begin / 1024;
+      fp.ntiles = (row_end + 1023) / 1024;
+      const uint64_t ctas = (fp.ntiles - fp.tile_begin + kFewWarps - 1) / kFewWarps;
+      const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)ctx->sm_count * 8));
+      switch (fp.ncols) {
+        case 1: batch_few_kernel<1><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 2: batch_few_kernel<2><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 3: batch_few_kernel<3><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 4: batch_few_kernel<4><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 5: batch_few_kernel<5><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 6: batch_few_kernel<6><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 7: batch_few_kernel<7><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        default: batch_few_kernel<8><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+      }
+      launches++;
+      continue;
+    }
+    const uint64_t rows_per_block = b.variant != 4    ? (uint64_t)(32 * kTilesPerBlock)
+                                    : b.groups == 16 ? (uint64_t)V4Shape<16>::kRows
+                                    : b.groups == 8  ? (uint64_t)V4Shape<8>::kRows
+                                                     : (uint64_t)V4Shape<4>::kRows;
     BatchPass bp = b.bp;
     bp.blob = dev_blob + b.off;
     bp.out = out;
@@ -690,8 +776,15 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
     if (b.variant == 4) {
-      if (b.cmax == 4) launch_one4<4>(bp, ctx->sm_count, s);
-      else launch_one4<8>(bp, ctx->sm_count, s);
+      if (b.cmax == 4) {
+        if (b.groups == 16) launch_one4<4, 16>(bp, ctx->sm_count, s);
+        else if (b.groups == 8) launch_one4<4, 8>(bp, ctx->sm_count, s);
+        else launch_one4<4, 4>(bp, ctx->sm_count, s);
+      } else {
+        if (b.groups == 16) launch_one4<8, 16>(bp, ctx->sm_count, s);
+        else if (b.groups == 8) launch_one4<8, 8>(bp, ctx->sm_count, s);
+        else launch_one4<8, 4>(bp, ctx->sm_count, s);
+      }
     } else if (b.cmax == 4) {
       if (w8) launch_one<4, 8>(bp, ctx->sm_count, s);
       else launch_one<4, 16>(bp, ctx->sm_count, s);

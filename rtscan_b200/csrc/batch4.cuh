@@ -1,39 +1,54 @@
-// Batched kernel, 512-query passes (included by batch.cu inside its
-// anonymous namespace; uses BatchPass, position() and kFull from there).
+// Batched kernel with table-driven passes of up to 512 queries (included by
+// batch.cu inside its anonymous namespace; uses BatchPass, position_fast(),
+// position() and kFull from there).
 //
-// A CTA of 16 warps works on blocks of 1024 rows (32 tiles of 32 rows) and
-// all 512 query slots of the pass (16 groups of 32) at once:
-//   1. every thread finds the interval positions of two rows (one per
+// A pass has GV groups of 32 query slots (GV = 16, 8 or 4: 512, 256 or 128
+// slots; the planner picks the smallest that holds the pass), and its
+// tables hold GV words per interval position.  A CTA of 16 warps works on
+// blocks of 32 x 512 / GV rows (1024, 2048, 4096): tiles of 32 rows, 32 / GV
+// tiles per warp, and all slots of the pass at once:
+//   1. every thread finds the interval positions of 32 / GV rows (one per
 //      column) and writes their table word offsets to shared memory, while
 //      the previous block's result words are stored;
-//   2. lane (tile t = 2*warp + lane/16, group g = lane%16) ANDs the table
-//      words of its tile's 32 rows for group g (one shared-memory load per
-//      row and column; the two tiles of a warp read two table rows), then
-//      bit-transposes the 32 masks in registers so that word j holds query
-//      32g+j's 32 row bits, MSB-first, and writes the 32 words to a
-//      shared-memory stage laid out [query][32 words] with word index
-//      tile ^ 2g, which puts the 32 lanes of a warp in 32 different banks;
-//   3. each warp stores 32 queries' rows of the stage: a query's 32 words
-//      (128 bytes, the block's 1024 rows) leave as eight 16-byte stores from
-//      eight lanes, one full 128-byte line per query.
-// No cross-lane exchange is needed, and positions are shared by all 512
-// queries of the pass.  Step 1 for the next block runs inside step 2 (see
-// the kernel), so one pair of barriers separates a block's steps.
+//   2. lane (tile t = (32 / GV) * warp + lane / GV, group g = lane % GV) ANDs
+//      the table words of its tile's 32 rows for group g (one shared-memory
+//      load per row and column), then bit-transposes the 32 masks in
+//      registers so that word j holds query 32g+j's 32 row bits, MSB-first,
+//      and writes the 32 words to a shared-memory stage laid out
+//      [query][tiles of the block] with word index t ^ ((32 / GV) * g),
+//      which puts the 32 lanes of a warp in 32 different banks;
+//   3. each warp stores 2 * GV queries' rows of the stage: a query's words
+//      for the block (128 bytes per 1024 rows) leave as 16-byte stores from
+//      128 / GV lanes, whole 128-byte lines.
+// No cross-lane exchange is needed, and positions are shared by all queries
+// of the pass.  For 512-slot passes over up to 4 columns, step 1 for the
+// next block runs inside step 2 (see the kernel).
 constexpr int kV4Warps = 16;
 constexpr int kV4Threads = kV4Warps * 32;
-constexpr int kV4Groups = 16;
-constexpr int kV4Slots = kV4Groups * 32;
-constexpr int kV4Tiles = 32;  // tiles per block
-constexpr int kV4Rows = kV4Tiles * 32;
-constexpr int kV4StageWords = kV4Slots * kV4Tiles;  // 64 KB
+constexpr int kV4StageWords = 16384;  // 64 KB: slots x words per query per block, for every GV
+constexpr int kV4MaxRows = 4096;      // rows per block of the smallest pass shape
+
+template <int GV>
+struct V4Shape {
+  static_assert(GV == 16 || GV == 8 || GV == 4, "512-, 256- or 128-slot passes");
+  static constexpr int kTPW = 32 / GV;               // tiles per warp
+  static constexpr int kTiles = kV4Warps * kTPW;     // tiles per block = words per query per block
+  static constexpr int kRows = kTiles * 32;          // rows per block
+  static constexpr int kSlots = 32 * GV;
+  static constexpr int kRPT = kRows / kV4Threads;    // rows per thread in step 1
+  static constexpr int kLPQ = 128 / GV;              // lanes per query row in step 3 (16-byte chunks)
+  static constexpr int kQPI = 32 / kLPQ;             // queries per store instruction
+  static_assert(kSlots * kTiles == kV4StageWords, "stage size");
+};
+
 // Per row and column the position buffer holds the word offset of the row's
-// table entry (table start + position * 16), to which a lane adds its group:
+// table entry (table start + position * GV), to which a lane adds its group:
 // 32-bit entries for up to 4 columns, 16-bit ones for 8 (a pass blob is
 // under 2^16 words), one padding row per tile.
 template <int CMAX>
 using V4Pos = typename std::conditional<(CMAX <= 4), uint32_t, uint16_t>::type;
-template <int CMAX>
-constexpr int kV4PosBytes = (kV4Rows + kV4Tiles) * CMAX * (int)sizeof(V4Pos<CMAX>);
+template <int CMAX, int GV>
+constexpr int kV4PosBytes = (V4Shape<GV>::kRows + V4Shape<GV>::kTiles) * CMAX * (int)sizeof(V4Pos<CMAX>);
 
 // Exchange the bits of a under mask M << S with the bits of b under M:
 // each result is one shift and one bitwise select.
@@ -77,8 +92,9 @@ __device__ __forceinline__ void transpose32(uint32_t (&x)[32]) {
   for (int i = 0; i < 32; i += 2) swap_bits<1, 0x55555555u>(x[i], x[i + 1]);
 }
 
-template <int CMAX>
+template <int CMAX, int GV>
 __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_constant__ BatchPass p) {
+  using S = V4Shape<GV>;
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t *blob = smem;
   uint32_t *stage = smem + ((p.blob_words + 3) & ~3u);
@@ -90,81 +106,123 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int C = p.ncols;
   const int32_t *slot_query = reinterpret_cast<const int32_t *>(blob + p.slot_off);
-  // compute-phase identity
-  const int tile = 2 * warp + (lane >> 4), g = lane & 15;
-  // store-phase identity: queries warp*32 + it*4 + qq, chunk c of 8
-  const int qq = lane >> 3, chunk = lane & 7;
-  const int pchunk = chunk ^ ((warp >> 1) & 7);  // physical 16-byte chunk of logical chunk `chunk`
-  const bool swap_pairs = warp & 1;              // words k and k^2 swapped inside a chunk
+  // step-2 identity
+  const int tile = S::kTPW * warp + lane / GV, g = lane % GV;
+  // step-3 identity: queries warp * 2GV + it * kQPI + qq, 16-byte chunk `chunk` of their row
+  const int qq = lane / S::kLPQ, chunk = lane % S::kLPQ;
+  const int sw = S::kTPW * (warp * GV / 16);  // stage word-index XOR of this warp's queries
+  const int pchunk = chunk ^ (sw >> 2);       // physical chunk of logical chunk `chunk`
+  const bool swap_pairs = sw & 2;             // words k and k^2 swapped inside a chunk
   uint32_t cnt[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) cnt[i] = 0;
 
-  // Positions are found one block ahead, inside the mask phase: even warps
-  // before their masks, odd warps after, so the dependent shared-memory
-  // loads of the boundary search overlap other warps' mask arithmetic.  The
-  // table word offsets wait in registers as 16-bit pairs until the next
-  // phase A writes them to the position buffer.  With up to 4 columns the
-  // column values are loaded one more block ahead.
-  constexpr bool kPrefetch = CMAX <= 4;
-  uint32_t val[2][CMAX];             // column values of this thread's two rows
-  uint32_t offn[2][(CMAX + 1) / 2];  // their table word offsets, two per register
+  // For 512-slot passes over up to 4 columns, positions are found one block
+  // ahead, inside step 2: even warps before their masks, odd warps after, so
+  // the dependent shared-memory loads of the boundary search overlap other
+  // warps' mask arithmetic; the table word offsets wait in registers as
+  // 16-bit pairs until the next step 1 writes them to shared memory, and the
+  // column values are loaded one more block ahead.  Other shapes find the
+  // positions of a block in its own step 1.
+  constexpr bool kAhead = GV == 16 && CMAX <= 4;
+  uint32_t val[S::kRPT][CMAX];                    // column values of this thread's rows
+  uint32_t offn[kAhead ? S::kRPT : 1][(CMAX + 1) / 2];  // their table word offsets, two per register
   auto load_values = [&](uint64_t b) {
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const uint64_t row = b * kV4Rows + threadIdx.x + h * kV4Threads;
+    for (int h = 0; h < S::kRPT; h++) {
+      const uint64_t row = b * S::kRows + threadIdx.x + h * kV4Threads;
 #pragma unroll
       for (int c = 0; c < CMAX; c++) val[h][c] = (c < C && row < p.nrows) ? __ldg(p.col[c] + row) : 0u;
     }
   };
-  auto find_offsets = [&](uint64_t b) {
+  auto row_offsets = [&](uint64_t b, int h, uint32_t(&off)[CMAX]) {
+    const bool in = b * S::kRows + threadIdx.x + h * kV4Threads < p.nrows;
+    uint32_t pos[CMAX];
+    if (kAhead) {  // latency hidden behind the masks: the search with the fewest instructions
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const bool in = b * kV4Rows + threadIdx.x + h * kV4Threads < p.nrows;
-      uint32_t off[CMAX];
+      for (int c = 0; c < CMAX; c++) pos[c] = (c < C && in) ? position(p, blob, c, val[h][c]) : 0u;
+    } else {  // loop-free lookups that overlap one another, full search when a bucket is crowded
+      bool exact = true;
 #pragma unroll
-      for (int c = 0; c < CMAX; c++)
-        off[c] = c < C ? p.tab_off[c] + (in ? position(p, blob, c, val[h][c]) : 0u) * kV4Groups : 0u;
+      for (int c = 0; c < CMAX; c++) {
+        bool e = true;
+        pos[c] = (c < C && in) ? position_fast(p, blob, c, val[h][c], e) : 0u;
+        exact = exact && e;
+      }
+      if (!exact) {
 #pragma unroll
-      for (int c = 0; c < CMAX; c += 2) offn[h][c / 2] = off[c] | (c + 1 < CMAX ? off[c + 1] << 16 : 0u);
+        for (int c = 0; c < CMAX; c++)
+          if (c < C) pos[c] = position(p, blob, c, val[h][c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[c] * GV : 0u;
+  };
+  auto put_row = [&](int h, const uint32_t(&off)[CMAX]) {
+    const int r = threadIdx.x + h * kV4Threads;
+    V4Pos<CMAX> *dst = posbuf + (r + (r >> 5)) * CMAX;
+    if (CMAX <= 4) {
+      *reinterpret_cast<uint4 *>(dst) = make_uint4(off[0], off[1 % CMAX], off[2 % CMAX], off[3 % CMAX]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < CMAX; c += 4)
+        *reinterpret_cast<uint2 *>(dst + c) =
+            make_uint2(off[c] | (off[(c + 1) % CMAX] << 16), off[(c + 2) % CMAX] | (off[(c + 3) % CMAX] << 16));
     }
   };
-  auto put_offsets = [&]() {
+  auto find_offsets = [&](uint64_t b) {  // kAhead: into offn
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int r = threadIdx.x + h * kV4Threads;
-      V4Pos<CMAX> *dst = posbuf + (r + (r >> 5)) * CMAX;
-      if (CMAX <= 4) {
-        *reinterpret_cast<uint4 *>(dst) = make_uint4(offn[h][0] & 0xFFFF, offn[h][0] >> 16,
-                                                     offn[h][1 % ((CMAX + 1) / 2)] & 0xFFFF,
-                                                     offn[h][1 % ((CMAX + 1) / 2)] >> 16);
-      } else {
+    for (int h = 0; h < S::kRPT; h++) {
+      uint32_t off[CMAX];
+      row_offsets(b, h, off);
 #pragma unroll
-        for (int c = 0; c < CMAX; c += 4)
-          *reinterpret_cast<uint2 *>(dst + c) = make_uint2(offn[h][c / 2], offn[h][c / 2 + 1]);
+      for (int c = 0; c < CMAX; c += 2) offn[h % (kAhead ? S::kRPT : 1)][c / 2] = off[c] | (c + 1 < CMAX ? off[c + 1] << 16 : 0u);
+    }
+  };
+  auto put_offsets = [&]() {  // kAhead: from offn
+#pragma unroll
+    for (int h = 0; h < S::kRPT; h++) {
+      uint32_t off[CMAX];
+#pragma unroll
+      for (int c = 0; c < CMAX; c++) {
+        const uint32_t w = offn[h % (kAhead ? S::kRPT : 1)][c / 2];
+        off[c] = (c & 1) ? w >> 16 : w & 0xFFFF;
       }
+      put_row(h, off);
     }
   };
 
   const uint64_t nblocks = p.nblocks, step = gridDim.x;
   uint64_t blk = p.block_begin + blockIdx.x;
   uint64_t prev = ~0ull;  // block whose stage is waiting to be stored
-  if (blk < nblocks) {
+  if (kAhead && blk < nblocks) {
     load_values(blk);
     find_offsets(blk);
-    if (kPrefetch && blk + step < nblocks) load_values(blk + step);
+    if (blk + step < nblocks) load_values(blk + step);
   }
   while (true) {
-    // ---- phase A: offsets of block `blk` to shared memory, store of block `prev` ----
-    if (blk < nblocks) put_offsets();
+    // ---- step 1: offsets of block `blk` to shared memory, store of block `prev` ----
+    if (blk < nblocks) {
+      if (kAhead) {
+        put_offsets();
+      } else {
+        load_values(blk);
+#pragma unroll
+        for (int h = 0; h < S::kRPT; h++) {
+          uint32_t off[CMAX];
+          row_offsets(blk, h, off);
+          put_row(h, off);
+        }
+      }
+    }
     if (prev != ~0ull) {
-      const uint64_t word0 = prev * kV4Tiles;
-      const bool full = p.vec_store && word0 + kV4Tiles <= p.words;
+      const uint64_t word0 = prev * S::kTiles;
+      const bool full = p.vec_store && word0 + S::kTiles <= p.words;
 #pragma unroll
       for (int it = 0; it < 8; it++) {
-        const int q = warp * 32 + it * 4 + qq;
+        const int q = warp * 2 * GV + it * S::kQPI + qq;
         const int32_t sq = slot_query[q];
-        uint4 v = *reinterpret_cast<const uint4 *>(stage + q * kV4Tiles + pchunk * 4);
+        uint4 v = *reinterpret_cast<const uint4 *>(stage + q * S::kTiles + pchunk * 4);
         if (swap_pairs) v = make_uint4(v.z, v.w, v.x, v.y);
         cnt[it] += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
         if (sq >= 0) {
@@ -182,18 +240,17 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
     }
     __syncthreads();
     if (blk >= nblocks) break;
-    // ---- phase B: masks, transpose, stage of `blk`; offsets of the next block ----
+    // ---- step 2: masks, transpose, stage of `blk` (and offsets of the next block) ----
     const uint64_t nxt = blk + step;
     auto ahead = [&]() {
-      if (nxt < nblocks) {
-        if (!kPrefetch) load_values(nxt);
+      if (kAhead && nxt < nblocks) {
         find_offsets(nxt);
-        if (kPrefetch && nxt + step < nblocks) load_values(nxt + step);
+        if (nxt + step < nblocks) load_values(nxt + step);
       }
     };
     if (!(warp & 1)) ahead();
     {
-      const uint64_t tile_row0 = blk * kV4Rows + (uint64_t)tile * 32;
+      const uint64_t tile_row0 = blk * S::kRows + (uint64_t)tile * 32;
       const uint32_t *tabg = blob + g;
       uint32_t acc[32];
 #pragma unroll
@@ -212,9 +269,9 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
           for (int c = 0; c < CMAX; c += 4) {
             const uint2 pv = *reinterpret_cast<const uint2 *>(pr + c);
             off[c] = pv.x & 0xFFFF;
-            off[c + 1] = pv.x >> 16;
-            off[c + 2] = pv.y & 0xFFFF;
-            off[c + 3] = pv.y >> 16;
+            off[(c + 1) % CMAX] = pv.x >> 16;
+            off[(c + 2) % CMAX] = pv.y & 0xFFFF;
+            off[(c + 3) % CMAX] = pv.y >> 16;
           }
         }
         uint32_t a = 0xFFFFFFFFu;
@@ -230,23 +287,22 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
 #pragma unroll
         for (int j = 0; j < 32; j++) acc[j] &= vm;
       }
-      const int col = tile ^ (2 * g);
+      const int col = tile ^ (S::kTPW * g);
 #pragma unroll
-      for (int j = 0; j < 32; j++) stage[(32 * g + j) * kV4Tiles + col] = acc[j];
+      for (int j = 0; j < 32; j++) stage[(32 * g + j) * S::kTiles + col] = acc[j];
     }
     if (warp & 1) ahead();
     __syncthreads();
     prev = blk;
     blk = nxt;
   }
-  // counts: lanes with the same qq hold partial counts of the same queries
+  // counts: the kLPQ lanes of a query row hold partial counts of that query
 #pragma unroll
   for (int it = 0; it < 8; it++) {
     uint32_t c = cnt[it];
-    c += __shfl_xor_sync(kFull, c, 1);
-    c += __shfl_xor_sync(kFull, c, 2);
-    c += __shfl_xor_sync(kFull, c, 4);
-    const int q = warp * 32 + it * 4 + qq;
+#pragma unroll
+    for (int o = 1; o < S::kLPQ; o <<= 1) c += __shfl_xor_sync(kFull, c, o);
+    const int q = warp * 2 * GV + it * S::kQPI + qq;
     const int32_t sq = slot_query[q];
     if (chunk == 0 && sq >= 0 && c) atomicAdd(p.counts + sq, (unsigned long long)c);
   }

@@ -335,7 +335,7 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
       if (cfg->segment_rows > 0) c.segment_rows = cfg->segment_rows;
       if (cfg->max_inflight_steps > 0) c.max_inflight_steps = cfg->max_inflight_steps;
     }
-    if (c.segment_rows % 1024) throw rts::Error(RTS_ERR_ARG, "segment_rows must be a multiple of 1024");
+    if (c.segment_rows % 4096) throw rts::Error(RTS_ERR_ARG, "segment_rows must be a multiple of 4096");
     srv->cfg = c;
     RTS_CUDA(cudaSetDevice(ctx->device));
     srv->nrows = ctx->nrows;

@@ -83,13 +83,36 @@ def test_batch_special_queries(ctx):
     check_batch(ctx, cols, qs)
 
 
-def test_batch_many_columns_per_pass(ctx):
-    """Queries over 6 different columns force passes with more than 4 table columns."""
-    n = 50_000
+@pytest.mark.parametrize("nq", [90, 200, 300])
+def test_batch_many_columns_per_pass(ctx, nq):
+    """Queries over 6 different columns force passes with more than 4 table
+    columns, in each pass shape (128, 256 and 512 query slots)."""
+    n = 50_000 + 4096 * 3 + 17
     cols = [D.uniform(n, 70 + c, 1 << (8 + 4 * c)) for c in range(6)]
     ctx.load_columns(cols)
-    qs = D.batch_queries(cols, 300, seed=11, min_cols=1, max_cols=6)
+    qs = D.batch_queries(cols, nq, seed=11, min_cols=1, max_cols=6)
     check_batch(ctx, cols, qs)
+
+
+def test_batch_few_pass_after_table_pass(ctx):
+    """520 queries over 7 columns: a 512-slot table pass, then an 8-query pass
+    tested term by term, both with more than 4 columns."""
+    n = 70_001
+    cols = [D.uniform(n, 600 + c, 1 << (6 + 4 * c)) for c in range(7)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 520, seed=13, min_cols=1, max_cols=7)
+    ctx.set_batch_config(4, 16, 512, 136 * 1024)
+    check_batch(ctx, cols, qs)
+
+
+@pytest.mark.parametrize("nq", [3, 128, 129, 256, 257])
+def test_batch_pass_shapes_at_block_edges(ctx, nq):
+    """Row counts one short of and one past the 1024-, 2048- and 4096-row
+    blocks of the three pass shapes."""
+    for n in (4095, 4097, 2 * 4096 + 2047, 3 * 4096 + 1025):
+        cols = [D.zipf(n, 400 + n, 1.2), D.normal(n, 401)]
+        ctx.load_columns(cols)
+        check_batch(ctx, cols, D.batch_queries(cols, nq, seed=n + nq))
 
 
 def test_batch_skewed_boundaries(ctx):
