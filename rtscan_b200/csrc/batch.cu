@@ -30,7 +30,6 @@
 #include <cmath>
 #include <cstring>
 #include <map>
-#include <set>
 #include <type_traits>
 #include <vector>
 
@@ -378,19 +377,19 @@ void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
 NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table) {
   NormQuery q;
   q.index = index;
-  std::vector<int> cols;
-  std::vector<uint32_t> lo, hi;
+  SmallVec<int, 16> cols;
+  SmallVec<uint32_t, 16> lo, hi;
   for (int i = 0; i < n; i++) {
     const rts_term &t = terms[i];
     if (t.column < 0 || t.column >= ncols_table) throw Error(RTS_ERR_ARG, "term column out of range");
     if (t.lo > t.hi) q.empty = true;
-    auto it = std::find(cols.begin(), cols.end(), (int)t.column);
+    const int *it = std::find(cols.begin(), cols.end(), (int)t.column);
     if (it == cols.end()) {
       cols.push_back(t.column);
       lo.push_back(t.lo);
       hi.push_back(t.hi);
     } else {
-      size_t k = it - cols.begin();
+      const size_t k = it - cols.begin();
       lo[k] = std::max(lo[k], t.lo);
       hi[k] = std::min(hi[k], t.hi);
       if (lo[k] > hi[k]) q.empty = true;
@@ -407,10 +406,43 @@ NormQuery normalize(const rts_term *terms, int n, int index, int ncols_table) {
 
 namespace {
 
+// Distinct nonzero boundary values of one pass column: open addressing for
+// membership, insertion order kept in `vals` (sorted when the pass closes).
+// Boundaries are never 0 (a lower bound of 0 and an upper bound of 2^32 - 1
+// constrain nothing), so 0 marks an empty cell.
+struct BoundSet {
+  std::vector<uint32_t> cell = std::vector<uint32_t>(64, 0u);
+  std::vector<uint32_t> vals;
+  uint32_t home(uint32_t v) const { return (v * 0x9E3779B1u) >> 7 & (uint32_t)(cell.size() - 1); }
+  bool has(uint32_t v) const {
+    for (uint32_t i = home(v);; i = (i + 1) & (uint32_t)(cell.size() - 1)) {
+      if (cell[i] == v) return true;
+      if (cell[i] == 0) return false;
+    }
+  }
+  void add(uint32_t v) {
+    if (has(v)) return;
+    if (2 * (vals.size() + 1) > cell.size()) {
+      cell.assign(cell.size() * 2, 0u);
+      for (uint32_t x : vals) put(x);
+    }
+    put(v);
+    vals.push_back(v);
+  }
+  size_t size() const { return vals.size(); }
+
+ private:
+  void put(uint32_t v) {
+    uint32_t i = home(v);
+    while (cell[i] != 0) i = (i + 1) & (uint32_t)(cell.size() - 1);
+    cell[i] = v;
+  }
+};
+
 struct PassPlan {
-  std::vector<int> qs;                      // normalized queries (indices into the list)
-  std::vector<int> cols;                    // table columns, in order
-  std::vector<std::set<uint32_t>> bounds;   // per table column
+  std::vector<int> qs;              // normalized queries (indices into the list)
+  std::vector<int> cols;            // table columns, in order
+  std::vector<BoundSet> bounds;     // per table column
 };
 
 // Shared-memory bytes of a pass's tables, boundaries and bucket index for
@@ -427,7 +459,7 @@ bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_pe
   if ((int)pp.qs.size() >= std::min(max_per_pass, 32 * G)) return false;
   size_t total = 0;
   int new_cols = 0;
-  std::vector<size_t> grow(pp.cols.size(), 0);
+  size_t grow[kMaxCols] = {0};
   for (size_t k = 0; k < q.cols.size(); k++) {
     auto it = std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]);
     size_t add = 0;
@@ -437,8 +469,8 @@ bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_pe
       total += column_bytes(add, G);
     } else {
       const auto &S = pp.bounds[it - pp.cols.begin()];
-      if (q.lo[k] > 0 && !S.count(q.lo[k])) grow[it - pp.cols.begin()]++;
-      if (q.hi[k] < 0xFFFFFFFFu && !S.count(q.hi[k] + 1)) grow[it - pp.cols.begin()]++;
+      if (q.lo[k] > 0 && !S.has(q.lo[k])) grow[it - pp.cols.begin()]++;
+      if (q.hi[k] < 0xFFFFFFFFu && !S.has(q.hi[k] + 1)) grow[it - pp.cols.begin()]++;
     }
   }
   if ((int)pp.cols.size() + new_cols > kMaxCols) return false;
@@ -454,8 +486,8 @@ bool try_add(PassPlan &pp, const NormQuery &q, int qi, size_t budget, int max_pe
     } else {
       ci = it - pp.cols.begin();
     }
-    if (q.lo[k] > 0) pp.bounds[ci].insert(q.lo[k]);
-    if (q.hi[k] < 0xFFFFFFFFu) pp.bounds[ci].insert(q.hi[k] + 1);
+    if (q.lo[k] > 0) pp.bounds[ci].add(q.lo[k]);
+    if (q.hi[k] < 0xFFFFFFFFu) pp.bounds[ci].add(q.hi[k] + 1);
   }
   pp.qs.push_back(qi);
   return true;
@@ -568,10 +600,11 @@ std::vector<uint16_t> bucket_index(const std::vector<uint32_t> &B, uint64_t span
   while ((span >> shift) > nb_target) shift++;
   const uint32_t nb = (uint32_t)(((span - 1) >> shift) + 1);  // buckets covering [bmin, bmax]
   std::vector<uint16_t> lin(nb + 1);
-  for (uint32_t k = 0; k <= nb; k++) {
+  uint32_t j = 0;
+  for (uint32_t k = 0; k <= nb; k++) {  // first boundary at or above the bucket's start
     const uint64_t start = (uint64_t)bmin + ((uint64_t)k << shift);
-    lin[k] = start > 0xFFFFFFFFull ? (uint16_t)m
-                                    : (uint16_t)(std::lower_bound(B.begin(), B.end(), (uint32_t)start) - B.begin());
+    while (j < m && (uint64_t)B[j] < start) j++;
+    lin[k] = (uint16_t)j;
   }
   *shift_out = shift;
   *lgm_out = 0;
@@ -651,42 +684,51 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     bp.ncols = C;
     std::vector<uint32_t> blob;
     std::vector<std::vector<uint32_t>> B(C);
-    for (int c = 0; c < C; c++) B[c].assign(pp.bounds[c].begin(), pp.bounds[c].end());
+    for (int c = 0; c < C; c++) {
+      B[c] = std::move(pp.bounds[c].vals);
+      std::sort(B[c].begin(), B[c].end());
+      bp.m[c] = (uint32_t)B[c].size();
+    }
     // tables: row pos holds, per slot, whether the values of interval pos
     // ([B[pos-1], B[pos]) with B[-1] = 0, B[m] = 2^32) pass the slot's term
     // on this column (always, when the slot does not constrain it).  Built
-    // as XOR deltas at the interval ends and a prefix XOR over positions.
+    // as XOR deltas at the interval ends and a prefix XOR over positions;
+    // a term [lo, hi] covers positions pos(lo) .. pos(hi) with pos(x) =
+    // #{B <= x}, where lo and hi + 1 are themselves boundaries.
+    std::vector<std::vector<uint32_t>> delta(C);
+    for (int c = 0; c < C; c++) delta[c].assign((size_t)(bp.m[c] + 2) * Gp, 0u);
+    std::vector<uint32_t> free_mask((size_t)C * Gp, 0u);  // slots leaving column c unconstrained
+    for (int slot = 0; slot < (int)pp.qs.size(); slot++) {
+      const uint32_t bit = 1u << (slot & 31);
+      const int grp = slot >> 5;
+      for (int c = 0; c < C; c++) free_mask[(size_t)c * Gp + grp] |= bit;
+      const NormQuery &q = norm[pp.qs[slot]];
+      for (size_t k = 0; k < q.cols.size(); k++) {
+        const int c = (int)(std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]) - pp.cols.begin());
+        const std::vector<uint32_t> &Bc = B[c];
+        const uint32_t m = bp.m[c];
+        const uint32_t p0 =
+            q.lo[k] > 0 ? (uint32_t)(std::lower_bound(Bc.begin(), Bc.end(), q.lo[k]) - Bc.begin()) + 1 : 0u;
+        const uint32_t p1 = q.hi[k] < 0xFFFFFFFFu
+                                ? (uint32_t)(std::lower_bound(Bc.begin(), Bc.end(), q.hi[k] + 1) - Bc.begin())
+                                : m;
+        delta[c][(size_t)p0 * Gp + grp] ^= bit;
+        delta[c][(size_t)(p1 + 1) * Gp + grp] ^= bit;
+        free_mask[(size_t)c * Gp + grp] &= ~bit;
+      }
+    }
     for (int c = 0; c < C; c++) {
-      const uint32_t m = (uint32_t)B[c].size();
-      bp.m[c] = m;
+      const uint32_t m = bp.m[c];
+      for (int grp = 0; grp < Gp; grp++) {  // unconstrained slots pass every position
+        delta[c][grp] ^= free_mask[(size_t)c * Gp + grp];
+        delta[c][(size_t)(m + 1) * Gp + grp] ^= free_mask[(size_t)c * Gp + grp];
+      }
       bp.tab_off[c] = (uint32_t)blob.size();
       blob.resize(blob.size() + (size_t)(m + 1) * Gp, 0u);
-      std::vector<uint32_t> delta((size_t)(m + 2) * Gp, 0u);
-      auto pos_of = [&](uint32_t x) {  // #boundaries <= x
-        return (uint32_t)(std::upper_bound(B[c].begin(), B[c].end(), x) - B[c].begin());
-      };
-      for (int slot = 0; slot < (int)pp.qs.size(); slot++) {
-        const NormQuery &q = norm[pp.qs[slot]];
-        auto it = std::find(q.cols.begin(), q.cols.end(), pp.cols[c]);
-        const uint32_t bit = 1u << (slot & 31);
-        const int grp = slot >> 5;
-        uint32_t p0 = 0, p1 = m;  // positions covered, inclusive
-        if (it != q.cols.end()) {
-          const size_t k = it - q.cols.begin();
-          p0 = pos_of(q.lo[k]);
-          p1 = pos_of(q.hi[k]);
-        }
-        delta[(size_t)p0 * Gp + grp] ^= bit;
-        delta[(size_t)(p1 + 1) * Gp + grp] ^= bit;
-      }
       uint32_t *tab = blob.data() + bp.tab_off[c];
-      for (int grp = 0; grp < Gp; grp++) {
-        uint32_t acc = 0;
-        for (uint32_t pos = 0; pos <= m; pos++) {
-          acc ^= delta[(size_t)pos * Gp + grp];
-          tab[(size_t)pos * Gp + grp] = acc;
-        }
-      }
+      uint32_t acc[32] = {0};
+      for (uint32_t pos = 0; pos <= m; pos++)
+        for (int grp = 0; grp < Gp; grp++) tab[(size_t)pos * Gp + grp] = acc[grp] ^= delta[c][(size_t)pos * Gp + grp];
     }
     // boundaries and bucket index
     for (int c = 0; c < C; c++) {

@@ -9,12 +9,45 @@
 
 namespace rts {
 
+// Vector with room for N elements in place, so that the usual query of a
+// few terms is planned without heap allocations; it moves to the heap when
+// it grows past N.
+template <class T, int N>
+class SmallVec {
+ public:
+  size_t size() const { return n_; }
+  bool empty() const { return n_ == 0; }
+  T *data() { return big_ ? heap_.data() : inl_; }
+  const T *data() const { return big_ ? heap_.data() : inl_; }
+  T *begin() { return data(); }
+  T *end() { return data() + n_; }
+  const T *begin() const { return data(); }
+  const T *end() const { return data() + n_; }
+  T &operator[](size_t i) { return data()[i]; }
+  const T &operator[](size_t i) const { return data()[i]; }
+  void push_back(const T &x) {
+    if (!big_ && n_ == (size_t)N) {
+      heap_.assign(inl_, inl_ + N);
+      big_ = true;
+    }
+    if (big_) heap_.push_back(x);
+    else inl_[n_] = x;
+    n_++;
+  }
+
+ private:
+  T inl_[N];
+  std::vector<T> heap_;
+  size_t n_ = 0;
+  bool big_ = false;
+};
+
 // A query after validation: terms merged per column (ranges intersected),
 // always-true terms dropped.
 struct NormQuery {
   int index = 0;                   // position in the caller's list
-  std::vector<int> cols;           // constrained columns
-  std::vector<uint32_t> lo, hi;
+  SmallVec<int, 8> cols;           // constrained columns
+  SmallVec<uint32_t, 8> lo, hi;
   bool empty = false;              // some term can never match
 };
 
@@ -42,7 +75,7 @@ BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, c
 // The words to upload to the device before launching.
 const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan);
 // Launch every pass over rows [row_begin, row_end) (row_begin a multiple of
-// 256) with the plan blob at dev_blob; counts are accumulated (not reset).
+// 4096) with the plan blob at dev_blob; counts are accumulated (not reset).
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out,
                       uint64_t stride_words, unsigned long long *counts, uint64_t row_begin, uint64_t row_end,
                       cudaStream_t s);
