@@ -1,31 +1,32 @@
 // Batched scan: many queries in one pass over the columns.
 //
 // The reference answers one query per loop iteration and re-reads its
-// columns every time (bindex_cuda.cpp:1827-1986).  Here a batch is answered
-// by persistent kernels that stream each column chunk from HBM once per
-// pass and evaluate up to 256 queries on it without per-query compares:
+// columns every time (bindex_cuda.cpp:1827-1986).  Here a batch is split
+// into passes of up to 512 queries over up to 8 constrained columns, and
+// each pass is one persistent kernel that streams every column chunk from
+// HBM once and evaluates all the pass's queries on it:
 //
 //   * Per pass and column, the host collects the query bounds on that
 //     column (lo and hi+1 of every term) into a sorted boundary list B.  The
 //     boundaries cut the value domain into intervals, and every query's
 //     verdict on the column is constant over an interval.  The kernel finds a
-//     row's interval ("position", #boundaries <= x) with a bucket index plus
-//     a short binary search, both in shared memory.
-//   * A mask table gives, per position, one bit per query (256 bits = eight
-//     32-bit words, one per group of 32 queries).  A row's verdict for all
-//     queries is the AND of its columns' table rows: C shared-memory loads
-//     per row and group instead of up to 2*C compares per row and query.
-//   * Lane (s, g) of a warp owns rows s*8..s*8+7 of a 32-row tile for query
-//     group g.  Its eight 32-bit masks are bit-transposed in registers (three
-//     delta-swap stages) into bytes, the four lanes of a group exchange
-//     bytes so that each finalizes 8 queries' 32-row words, and the words
-//     are staged in shared memory (a rotated layout that is bank-conflict
-//     free on both sides) until eight tiles make a full 32-byte sector per
-//     query, which the warp then stores with coalesced writes.
+//     row's interval ("position", #boundaries <= x) with a bucket index
+//     (linear or log-linear buckets, whichever spreads this column's
+//     boundaries better) plus a short search, all in shared memory.
+//   * A mask table gives, per position, one bit per query slot (G words of
+//     32 slots).  A row's verdict for all queries is the AND of its columns'
+//     table rows: C shared-memory loads per row and group of 32 queries
+//     instead of up to 2*C compares per row and query.
+//   * Variant 4 (default, batch4.cuh): CTA-wide blocks of 1024-4096 rows;
+//     each lane ANDs the masks of 32 rows for one group, transposes the
+//     32x32 bit block in registers and stages the words for whole-line
+//     stores.  Passes of at most 32 queries skip the tables and test each
+//     term directly (batch_few.cuh).  Variant 3 (below): 256-query passes
+//     with one 256-row block per warp, kept as an autotuner candidate.
 //   * Counts are kept per lane in registers and flushed once per CTA.
 // Queries with an empty term, with no constrained column, or with more than
-// eight constrained columns are answered outside this kernel (fill or fused
-// scan), so the result of every query equals the single-query path.
+// eight constrained columns are answered outside these kernels (fill or
+// fused scan), so the result of every query equals the single-query path.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -162,6 +163,13 @@ __device__ __forceinline__ uint32_t stage_index(uint32_t slot, uint32_t t) {
   return row * 32 + col;
 }
 
+// Variant 3: 256-slot passes (8 groups), one 256-row block per warp.  Lane
+// (s, g) owns rows s*8..s*8+7 of a 32-row tile for query group g; its eight
+// 32-bit masks are bit-transposed in registers (three delta-swap stages)
+// into bytes, the four lanes of a group exchange bytes so that each
+// finalizes 8 queries' 32-row words, and the words are staged in shared
+// memory until eight tiles make a full 32-byte sector per query, which the
+// warp then stores with coalesced writes.
 // CMAX: columns a pass may constrain (4 or 8); W: warps per CTA (8 or 16).
 template <int CMAX, int W>
 __global__ void __launch_bounds__(W * 32, 16 / W) batch_kernel(const __grid_constant__ BatchPass p) {
