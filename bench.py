@@ -440,6 +440,9 @@ def run(args):
         line["batch_config"]["source"] = "autotuned" if tuned else "default"
     line.update(extra)
 
+    if wl == "batched" and args.pass_sweep:
+        line["pass_sweep"] = pass_sweep(torch, R, D, dev, rank, args.pass_sweep)
+
     if wl == "batched" and not args.no_serve:
         del out, cnt
         ctx.attach_columns([c.data_ptr() for c in cols[:1]], n)
@@ -475,6 +478,41 @@ def run(args):
 
 
 SERVE_KINDS = ["uniform", "uniform", "zipf1.3", "zipf1.3"]
+
+
+def pass_sweep(torch, R, D, dev, rank, n, sizes=(1, 4, 16, 64, 128, 256, 512)):
+    """Kernel time of one pass of each size over an n-row table of the served
+    kinds (one server segment): a prepared batch (CUDA graph) replayed 7
+    times, median CUDA-event time on the launching stream."""
+    cols = [gpu_column(torch, k, n, 7000 * (rank + 1) + i, dev) for i, k in enumerate(SERVE_KINDS)]
+    samples = [host_sample(torch, c, seed=21 + i) for i, c in enumerate(cols)]
+    ctx = R.Context(dev.index or 0)
+    ctx.attach_columns([c.data_ptr() for c in cols], n)
+    stride = (R.bitmap_words(n) + 31) // 32 * 32
+    s = torch.cuda.current_stream()
+    out = []
+    for nq in sizes:
+        qs = D.batch_queries(samples, nq, seed=nq)
+        bm = torch.empty(nq * stride, dtype=torch.int32, device=dev)
+        cnt = torch.zeros(nq, dtype=torch.int64, device=dev)
+        pb = ctx.prepare_batch(qs, bm.data_ptr(), stride, cnt.data_ptr())
+        for _ in range(3):
+            pb.launch(s.cuda_stream)
+        ts = []
+        for _ in range(7):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            pb.launch(s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        pb.release()
+        ms = statistics.median(ts)
+        out.append({"queries": nq, "us": round(1e3 * ms, 1), "us_per_query": round(1e3 * ms / nq, 2)})
+        del bm, cnt
+    ctx.close()
+    del cols
+    return {"rows": n, "kinds": SERVE_KINDS, "passes": out}
 
 
 def served_leg(torch, R, D, ctx, dev, rank, args):
@@ -573,6 +611,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the one-query-per-launch comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-scan leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch launch shape")
+    ap.add_argument("--pass-sweep", type=int, default=0, metavar="ROWS",
+                    help="also time one pass of 1..512 queries over a ROWS-row table (off by default)")
     ap.add_argument("--serve-rows", type=int, default=1 << 28)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[1000, 5000, 10000])
     ap.add_argument("--serve-seconds", type=float, default=2.0)
