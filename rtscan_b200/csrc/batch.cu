@@ -933,13 +933,14 @@ struct HostBatchBuffers {
   size_t bm_cap = 0;
   unsigned long long *counts = nullptr;
   size_t cnt_cap = 0;
-  cudaStream_t compute = nullptr, copy = nullptr;
+  cudaStream_t up = nullptr, compute = nullptr, copy = nullptr;
   std::vector<cudaEvent_t> ev;
   ~HostBatchBuffers() {
     if (cols) cudaFree(cols);
     if (bitmaps) cudaFree(bitmaps);
     if (counts) cudaFree(counts);
     for (auto e : ev) cudaEventDestroy(e);
+    if (up) cudaStreamDestroy(up);
     if (compute) cudaStreamDestroy(compute);
     if (copy) cudaStreamDestroy(copy);
   }
@@ -979,14 +980,13 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
     if (!ctx->host_batch) ctx->host_batch = new rts::HostBatchBuffers();
     rts::HostBatchBuffers &H = *ctx->host_batch;
+    if (!H.up) RTS_CUDA(cudaStreamCreateWithFlags(&H.up, cudaStreamNonBlocking));
     if (!H.compute) RTS_CUDA(cudaStreamCreateWithFlags(&H.compute, cudaStreamNonBlocking));
     if (!H.copy) RTS_CUDA(cudaStreamCreateWithFlags(&H.copy, cudaStreamNonBlocking));
     const uint64_t cstride = (nrows + 3) / 4 * 4;
     rts::ensure(H.cols, H.cols_cap, (size_t)cstride * ncols);
     rts::ensure(H.bitmaps, H.bm_cap, (size_t)std::max(nq, 1) * stride_words);
     rts::ensure(H.counts, H.cnt_cap, (size_t)std::max(nq, 1));
-    for (int c = 0; c < ncols; c++)
-      RTS_CUDA(cudaMemcpyAsync(H.cols + cstride * c, host_cols[c], nrows * 4, cudaMemcpyHostToDevice, H.compute));
     // The batch kernels read the uploaded columns through the context.
     std::vector<const uint32_t *> saved_cols = ctx->cols;
     const uint64_t saved_n = ctx->nrows;
@@ -1002,28 +1002,65 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
         c->nrows = n;
       }
     } restore{ctx, saved_cols, saved_n};
-    const int chunk = 256;
-    const int nchunks = (nq + chunk - 1) / chunk;
-    while ((int)H.ev.size() < nchunks) {
+    // Row-chunked pipeline over three streams: the upload of chunk r+1 and
+    // the download of chunk r-1's words of every bitmap (one 2D copy) run
+    // while chunk r is scanned, so the column upload hides under the bitmap
+    // download.  Chunks are multiples of 4096 rows (the largest kernel block).
+    std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms, offsets, nq);
+    std::vector<int> inside, outside;
+    for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
+    const uint64_t want_chunks = std::max<uint64_t>(1, std::min<uint64_t>(8, nrows >> 22));
+    const uint64_t chunk_rows = ((nrows + want_chunks - 1) / want_chunks + 4095) / 4096 * 4096;
+    const int nchunks = (int)((nrows + chunk_rows - 1) / chunk_rows);
+    while ((int)H.ev.size() < 2 * nchunks + 1) {
       cudaEvent_t e;
       RTS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       H.ev.push_back(e);
     }
-    for (int k = 0; k < nchunks; k++) {
-      const int q0 = k * chunk, q1 = std::min(nq, q0 + chunk);
-      std::vector<int32_t> off(offsets + q0, offsets + q1 + 1);
-      for (auto &o : off) o -= offsets[q0];
-      rts::batch_scan(ctx, terms + offsets[q0], off.data(), q1 - q0, H.bitmaps + (uint64_t)q0 * stride_words,
-                      stride_words, H.counts + q0, H.compute, ctx->batch_cfg.table_budget);
-      RTS_CUDA(cudaEventRecord(H.ev[k], H.compute));
-      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[k], 0));
-      RTS_CUDA(cudaMemcpyAsync(host_bitmaps + (uint64_t)q0 * stride_words, H.bitmaps + (uint64_t)q0 * stride_words,
-                               (uint64_t)(q1 - q0) * stride_words * 4, cudaMemcpyDeviceToHost, H.copy));
+    if (nq > 0) RTS_CUDA(cudaMemsetAsync(H.counts, 0, (size_t)nq * 8, H.compute));
+    rts::BatchPlan plan;
+    const uint32_t *dev_blob = nullptr;
+    cudaEvent_t blob_done = nullptr;
+    if (!inside.empty()) {
+      plan = rts::build_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget);
+      dev_blob = rts::upload_plan(ctx, plan, H.compute, &blob_done);
     }
-    if (nq > 0)
+    for (int r = 0; r < nchunks; r++) {
+      const uint64_t r0 = (uint64_t)r * chunk_rows, r1 = std::min<uint64_t>(nrows, r0 + chunk_rows);
+      for (int c = 0; c < ncols; c++)
+        RTS_CUDA(cudaMemcpyAsync(H.cols + cstride * c + r0, host_cols[c] + r0, (r1 - r0) * 4,
+                                 cudaMemcpyHostToDevice, H.up));
+      RTS_CUDA(cudaEventRecord(H.ev[2 * r], H.up));
+      RTS_CUDA(cudaStreamWaitEvent(H.compute, H.ev[2 * r], 0));
+      if (!inside.empty())
+        ctx->launches += rts::launch_plan(ctx, plan, dev_blob, H.bitmaps, stride_words, H.counts, r0, r1, H.compute);
+      RTS_CUDA(cudaEventRecord(H.ev[2 * r + 1], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * r + 1], 0));
+      const uint64_t w0 = r0 / 32, w1 = r1 == nrows ? words : r1 / 32;
+      if (nq > 0)
+        RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + w0, stride_words * 4, H.bitmaps + w0, stride_words * 4,
+                                   (w1 - w0) * 4, (size_t)nq, cudaMemcpyDeviceToHost, H.copy));
+    }
+    // Queries outside the batch kernels read the whole table: after the last
+    // upload (ordered on the compute stream), then their whole bitmaps.
+    if (!outside.empty()) {
+      ctx->launches += rts::launch_outside(ctx, norm, outside, nullptr, H.bitmaps, stride_words, H.counts, H.compute);
+      RTS_CUDA(cudaEventRecord(H.ev[2 * nchunks], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * nchunks], 0));
+      for (int q : outside)
+        RTS_CUDA(cudaMemcpyAsync(host_bitmaps + (uint64_t)q * stride_words, H.bitmaps + (uint64_t)q * stride_words,
+                                 words * 4, cudaMemcpyDeviceToHost, H.copy));
+    }
+    if (blob_done) RTS_CUDA(cudaEventRecord(blob_done, H.compute));
+    RTS_CUDA(cudaGetLastError());
+    if (nq > 0) {
+      RTS_CUDA(cudaEventRecord(H.ev[2 * nchunks], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * nchunks], 0));
       RTS_CUDA(cudaMemcpyAsync(host_counts, H.counts, (size_t)nq * 8, cudaMemcpyDeviceToHost, H.copy));
+    }
     RTS_CUDA(cudaStreamSynchronize(H.copy));
     RTS_CUDA(cudaStreamSynchronize(H.compute));
+    RTS_CUDA(cudaStreamSynchronize(H.up));
     if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {

@@ -214,6 +214,27 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
         ctx.set_batch_config(4, 16, 513, 88 * 1024)
 
 
+@pytest.mark.parametrize("n", [70_001, 9_000_011])
+def test_batch_host_buffers(ctx, n):
+    """Host columns in, host bitmaps out: the upload, scan and download run as
+    a row-chunked pipeline (two chunks at 9e6 rows), with queries outside the
+    batch kernels (no term, an empty term, nine columns) among them.  The
+    context's own table is untouched."""
+    ctx.load_columns([D.uniform(1000, 1)])
+    cols = [D.uniform(n, 500 + c, [1 << 32, 1 << 20, 4096, 256, 64, 1 << 16, 1 << 32, 1000, 77][c])
+            for c in range(9)]
+    cols[2] = D.zipf(n, 502, 1.3)
+    qs = D.batch_queries(cols[:4], 300, seed=17) + [
+        [], [(3, 9, 2)], [(c, 1, [1 << 31, 1 << 19, 4000, 200, 60, 1 << 15, 1 << 31, 900, 70][c]) for c in range(9)]]
+    stride = R.bitmap_words(n) + 3
+    bms, counts = ctx.scan_batch_host(cols, qs, stride_words=stride)
+    for i, q in enumerate(qs):
+        want, wcnt = expect(cols, q)
+        assert int(counts[i]) == wcnt, (i, q)
+        assert np.array_equal(bms[i, :R.bitmap_words(n)], want), (i, q)
+    assert ctx.nrows == 1000
+
+
 def test_prepared_batch_graph_replays_match(ctx):
     n = 333_333
     cols = [D.uniform(n, 300), D.zipf(n, 301, 1.5), D.uniform(n, 302, 64)]
