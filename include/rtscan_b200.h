@@ -313,6 +313,31 @@ RTS_API rts_status rts_server_stop(rts_server *srv);
 RTS_API rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets,
                                      int32_t nqueries, const double *arrival_s, double *latency_ms);
 
+/* ---- after the scan: row ids and aggregates --------------------------------- */
+/* No reference counterpart: the reference stops at the bitmap and its hit
+ * count, and its query files name the step that follows in a query engine
+ * (TPC-H Q6, a filtered sum of l_extendedprice * l_discount,
+ * test/scan_cmd_1e8-1c.txt:48-54). */
+
+/* Ascending row ids of the set bits of an MSB-first bitmap of nrows bits
+ * (nrows < 2^32; bits past nrows are ignored): at most `capacity` ids are
+ * written to dev_rows, and *dev_count gets the number of set bits, so a
+ * caller whose buffer was too small can size it and call again. */
+RTS_API rts_status rts_bitmap_rows_async(rts_ctx *ctx, const uint32_t *dev_bitmap, uint64_t nrows,
+                                         uint32_t *dev_rows, uint64_t capacity, uint64_t *dev_count,
+                                         void *stream);
+/* Sum over the set rows of dev_bitmap (rts_nrows(ctx) bits) of resident
+ * column col_a, or of col_a x col_b when col_b >= 0: an exact 128-bit value
+ * in dev_sum[0] (low 64 bits) and dev_sum[1] (high 64 bits). */
+RTS_API rts_status rts_bitmap_sum_async(rts_ctx *ctx, const uint32_t *dev_bitmap, int32_t col_a, int32_t col_b,
+                                        uint64_t *dev_sum, void *stream);
+/* A conjunctive query and its aggregate in one pass, with no bitmap: the
+ * hit count in *dev_count (may be NULL) and, when col_a >= 0, the 128-bit
+ * sum of col_a (col_b < 0) or of col_a x col_b over the hits in dev_sum[0..1].
+ * At most 8 distinct columns between the terms and the aggregate. */
+RTS_API rts_status rts_scan_aggregate_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, int32_t col_a,
+                                            int32_t col_b, uint64_t *dev_count, uint64_t *dev_sum, void *stream);
+
 /* ---- allocation-free scan ------------------------------------------------ */
 
 /* Largest row count rts_scan_separate_noalloc_async accepts (2^27 rows; its

@@ -118,6 +118,10 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_bitmap_rows_async", ctypes.c_int32, [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P, _P]),
+    ("rts_bitmap_sum_async", ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P]),
+    ("rts_scan_aggregate_async", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P,
+                                                  _P, _P]),
     ("rts_batch_prepare", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P,
                                            ctypes.c_uint64, _P, ctypes.POINTER(_P)]),
     ("rts_batch_launch", ctypes.c_int32, [_P, _P]),
@@ -424,6 +428,22 @@ class Context:
     def scan_async(self, terms, bitmap_ptr: int, count_ptr: int, stream: int = 0) -> None:
         arr, n = make_terms(terms)
         self._c(lib().rts_scan_async(self._h, arr, n, bitmap_ptr, count_ptr, stream))
+
+    def bitmap_rows_async(self, bitmap_ptr: int, nrows: int, rows_ptr: int, capacity: int, count_ptr: int,
+                          stream: int = 0) -> None:
+        """Ascending uint32 row ids of the set bits (at most `capacity`)."""
+        self._c(lib().rts_bitmap_rows_async(self._h, bitmap_ptr, nrows, rows_ptr, capacity, count_ptr, stream))
+
+    def bitmap_sum_async(self, bitmap_ptr: int, col_a: int, col_b: int, sum_ptr: int, stream: int = 0) -> None:
+        """128-bit sum of column col_a (x col_b when col_b >= 0) over the set
+        rows, as two uint64 words (low, high) at sum_ptr."""
+        self._c(lib().rts_bitmap_sum_async(self._h, bitmap_ptr, col_a, col_b, sum_ptr, stream))
+
+    def scan_aggregate_async(self, terms, col_a: int, col_b: int, count_ptr: int, sum_ptr: int,
+                             stream: int = 0) -> None:
+        """Query and aggregate in one pass, no bitmap."""
+        arr, n = make_terms(terms)
+        self._c(lib().rts_scan_aggregate_async(self._h, arr, n, col_a, col_b, count_ptr, sum_ptr, stream))
 
     def scan_separate_async(self, terms, bitmap_ptr: int, count_ptr: int, stream: int = 0) -> None:
         arr, n = make_terms(terms)

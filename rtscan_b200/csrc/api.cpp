@@ -191,6 +191,7 @@ rts_ctx::~rts_ctx() {
   if (plan_dev) cudaFree(plan_dev);
   if (plan_host) cudaFreeHost(plan_host);
   if (small_dev) cudaFree(small_dev);
+  if (agg_dev) cudaFree(agg_dev);
   if (batch) rts::destroy_batch(batch);
   if (host_batch) rts::destroy_host_batch(host_batch);
 }

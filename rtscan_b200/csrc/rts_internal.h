@@ -131,6 +131,8 @@ struct rts_ctx {
   size_t plan_bytes = 0;
   void *plan_host = nullptr;  // pinned
   void *small_dev = nullptr;
+  void *agg_dev = nullptr;    // compaction scratch (tile counts and offsets)
+  size_t agg_bytes = 0;
   rts::BatchScratch *batch = nullptr;
   rts::HostBatchBuffers *host_batch = nullptr;
   rts::BatchConfig batch_cfg;
