@@ -1,7 +1,7 @@
 """Benchmark driver: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload batched|single|multi] [--nrows N] [--queries Q]
+                    [--workload batched|single|multi|q6] [--nrows N] [--queries Q]
 
 Workloads (seeded synthetic data generated on the device; no dataset is read):
   batched  (default) 1e8 rows x 4 uint32 columns (zipf 1.1, 1.3, 1.5 over 2^20
@@ -14,6 +14,12 @@ Workloads (seeded synthetic data generated on the device; no dataset is read):
            = one fused scan launch.
   multi    1e8 rows x 4 uniform columns, one conjunctive query with
            per-column selectivity in [5%, 50%]; fused vs separate passes.
+  q6       1e8 rows x 4 integer-coded columns shaped like TPC-H Q6
+           (shipdate, discount, quantity, extendedprice); one step = one
+           fused scan-and-aggregate (count and sum of price x discount over
+           shipdate in 1994, discount 5-7, quantity < 24), no bitmap.
+           Compared with the scan followed by the masked sum, and with the
+           compaction of its bitmap to row ids.
 
 Under torchrun each rank scans its own rows (weak scaling, no collective on
 the data path); `value` is the aggregate over ranks.  Timing: W warm-up
@@ -39,7 +45,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "batched range-scan GB/s & queries/s vs HBM peak; served query p50/p99 ms"
+Q6_METRIC = "fused scan-and-aggregate GB/s vs HBM peak"
 BATCH_KINDS = ["zipf1.1", "zipf1.3", "zipf1.5", "normal"]
+# TPC-H Q6 shape, integer-coded: shipdate (yyyymmdd-like), discount (%),
+# quantity, extendedprice (cents)
+Q6_KINDS = ["range:19920101:19990101", "range:0:11", "range:1:51", "range:90000:10500000"]
+Q6_TERMS = [(0, 19940101, 19950100), (1, 5, 7), (2, 0, 23)]
 
 
 # ----------------------------------------------------------------------------
@@ -152,6 +163,9 @@ def gpu_column(torch, kind: str, n: int, seed: int, device):
     if kind == "uniform":
         x = torch.randint(0, 1 << 32, (n,), generator=g, device=device, dtype=torch.int64)
         return x.to(torch.int32)  # two's-complement wrap keeps the uint32 bit pattern
+    if kind.startswith("range:"):  # uniform integers in [a, b)
+        a, b = (int(x) for x in kind.split(":")[1:])
+        return torch.randint(a, b, (n,), generator=g, device=device, dtype=torch.int64).to(torch.int32)
     out = torch.empty(n, dtype=torch.int32, device=device)
     chunk = 1 << 24
     if kind.startswith("zipf"):
@@ -185,6 +199,8 @@ def make_queries(D, wl, samples, nq, seed=42):
     rng = np.random.default_rng(seed)
     if wl == "single":
         return [[(0, *D.range_for_selectivity(samples[0], 0.10))]]
+    if wl == "q6":
+        return [list(Q6_TERMS)]
     if wl == "multi":
         q = []
         for c in range(len(samples)):
@@ -259,7 +275,34 @@ def cpu_reference_run(cols_np, queries, repeats=3, max_seconds=60.0):
 
 def cpu_sample_columns(kinds, m):
     from rtscan_b200 import datagen as D
-    return [D.column(k, m, 1000 + i) for i, k in enumerate(kinds)]
+    out = []
+    for i, k in enumerate(kinds):
+        if k.startswith("range:"):
+            a, b = (int(x) for x in k.split(":")[1:])
+            out.append(np.random.default_rng(1000 + i).integers(a, b, m).astype(np.uint32))
+        else:
+            out.append(D.column(k, m, 1000 + i))
+    return out
+
+
+def q6_cpu_port(kinds, terms):
+    """The q6 step restated in numpy (one thread) on REF_N rows: the
+    reference has no aggregate step to time."""
+    cols = cpu_sample_columns(kinds, REF_N)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        hit = np.ones(REF_N, bool)
+        for c, lo, hi in terms:
+            hit &= (cols[c] >= lo) & (cols[c] <= hi)
+        total = int(np.sum(cols[3][hit].astype(np.uint64) * cols[1][hit].astype(np.uint64)))
+        reps += 1
+        if time.perf_counter() - t0 > 3.0:
+            break
+    sec = (time.perf_counter() - t0) / reps
+    return {"value": round(4 * REF_N * len(cols) / sec / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+            "sample": f"{REF_N} rows x {len(cols)} columns, numpy restatement of the q6 step "
+                      f"({reps} repetitions; sum {total})"}
 
 
 # ----------------------------------------------------------------------------
@@ -286,7 +329,7 @@ def run(args):
 
     n = args.nrows
     wl = args.workload
-    kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, BATCH_KINDS)
+    kinds = {"single": ["uniform"], "multi": ["uniform"] * 4, "q6": Q6_KINDS}.get(wl, BATCH_KINDS)
     cols = [gpu_column(torch, k, n, 1000 * (rank + 1) + i, dev) for i, k in enumerate(kinds)]
     ctx.attach_columns([c.data_ptr() for c in cols], n)
     samples = [host_sample(torch, c, seed=7 + i) for i, c in enumerate(cols)]
@@ -297,12 +340,16 @@ def run(args):
     stride = (words + 31) // 32 * 32
     out = torch.empty(nq * stride, dtype=torch.int32, device=dev)
     cnt = torch.zeros(nq, dtype=torch.int64, device=dev)
-    bytes_step = step_bytes(n, queries)
+    bytes_step = step_bytes(n, queries) if wl != "q6" else 4 * n * len(cols)
+    agg_cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    agg_sum = torch.zeros(2, dtype=torch.int64, device=dev)
     tuned = None
     if wl == "batched" and not args.no_autotune:
         tuned = ctx.autotune_batch(pq)  # launch shape for this table and batch (outside the timed region)
     if wl == "batched":
         launch = lambda: ctx.scan_batch_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s)
+    elif wl == "q6":
+        launch = lambda: ctx.scan_aggregate_async(queries[0], 3, 1, agg_cnt.data_ptr(), agg_sum.data_ptr(), s)
     else:
         launch = lambda: ctx.scan_async(queries[0], out.data_ptr(), cnt.data_ptr(), s)
 
@@ -356,6 +403,8 @@ def run(args):
         per_g, _ = timed(lambda: pb.launch(s), args.steps)
         extra["graph_replay_ms_per_step"] = round(statistics.median(per_g), 4)
         pb.release()
+    if wl == "q6":
+        extra.update(q6_legs(torch, R, ctx, queries[0], n, out, cnt, s, timed, statistics.median(per)))
     if world > 1:
         from rtscan_b200 import shard as SH
         extra["global_match_count_q0"] = int(SH.all_reduce_counts(cnt[:1].cpu().numpy())[0])
@@ -383,7 +432,9 @@ def run(args):
     # e2e through the C-ABI with host buffers: the step's columns uploaded
     # from pinned host memory and every result bitmap + count read back.
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and wl == "q6":
+        e2e = q6_e2e(torch, R, local, cols, queries[0], bytes_step, world, dev, barrier)
+    elif not args.no_e2e:
         host_cols = [c.cpu().pin_memory() for c in cols]
         host_np = [h.numpy().view(np.uint32) for h in host_cols]
         hb = torch.empty((nq, stride), dtype=torch.int32).pin_memory()
@@ -407,7 +458,7 @@ def run(args):
 
     gbs_total = bytes_step * world / (ms_step * 1e-3) / 1e9
     line = {
-        "metric": METRIC,
+        "metric": METRIC if wl != "q6" else Q6_METRIC,
         "value": round(gbs_total, 2),
         "unit": "GB/s",
         "n_gpus": world,
@@ -421,7 +472,8 @@ def run(args):
         "data": "synthetic (seeded, generated on device)",
         "config": {"workload": {"batched": f"batched scan {n:.3g} rows x 4 skewed columns, {nq} queries",
                                 "single": f"single-column {n:.3g}-row scan, 10% selectivity",
-                                "multi": f"4-column {n:.3g}-row conjunctive scan"}[wl],
+                                "multi": f"4-column {n:.3g}-row conjunctive scan",
+                                "q6": f"fused scan-and-aggregate, {n:.3g} rows x 4 columns (TPC-H Q6 shape)"}[wl],
                    "nrows_per_gpu": n, "ncols": len(cols), "queries_per_step": nq,
                    "column_kinds": kinds, "l2": f"inputs larger than L2 ({n * 4 / 1e6:.0f} MB per column)"},
         "queries_per_s": round(nq * world / (ms_step * 1e-3), 1),
@@ -456,7 +508,9 @@ def run(args):
             line["served_p99_ms"] = ref["p99_ms"]
             line["served_at_qps"] = ref["offered_qps"]
 
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and wl == "q6":
+        line["cpu_baseline"] = q6_cpu_port(kinds, queries[0])
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
         cols_np = cpu_sample_columns(kinds, REF_N)
         smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols_np]
         qs = make_queries(D, wl, smp, args.queries)[: 16]
@@ -475,6 +529,64 @@ def run(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def q6_legs(torch, R, ctx, terms, n, out, cnt, s, timed, fused_ms):
+    """The q6 step the long way (scan to a bitmap, then the masked sum), and
+    the compaction of that bitmap to row ids, each timed like the step."""
+    dev = out.device
+    sm = torch.zeros(2, dtype=torch.int64, device=dev)
+    rc = torch.zeros(1, dtype=torch.int64, device=dev)
+    bm = out.data_ptr()
+
+    def two_pass():
+        ctx.scan_async(terms, bm, cnt.data_ptr(), s)
+        ctx.bitmap_sum_async(bm, 3, 1, sm.data_ptr(), s)
+    two_pass()
+    per2, _ = timed(two_pass, 5)
+    hits = int(cnt[0].item())
+    rows = torch.empty(max(1, hits), dtype=torch.int32, device=dev)
+    compact = lambda: ctx.bitmap_rows_async(bm, n, rows.data_ptr(), hits, rc.data_ptr(), s)
+    compact()
+    perc, _ = timed(compact, 5)
+    msum = lambda: ctx.bitmap_sum_async(bm, 3, 1, sm.data_ptr(), s)
+    msum()
+    pers, _ = timed(msum, 5)
+    m2, mc, ms = statistics.median(per2), statistics.median(perc), statistics.median(pers)
+    words = (n + 31) // 32
+    return {"hits": hits,
+            "scan_then_masked_sum_ms": round(m2, 4), "fused_speedup_vs_two_pass": round(m2 / fused_ms, 3),
+            "masked_sum": {"ms": round(ms, 4), "GB_s": round((words * 4 + 8 * n) / (ms * 1e-3) / 1e9, 1),
+                           "bytes": "bitmap + 2 columns"},
+            "bitmap_to_rows": {"ms": round(mc, 4), "rows": hits,
+                               "GB_s": round((2 * words * 4 + 4 * hits) / (mc * 1e-3) / 1e9, 1),
+                               "bytes": "bitmap twice + 4 per row id"}}
+
+
+def q6_e2e(torch, R, local, cols, terms, bytes_step, world, dev, barrier):
+    """q6 through the public API from host memory: upload the 4 pinned
+    columns into a context, run the fused scan-and-aggregate, read the count
+    and sum back."""
+    host = [c.cpu().pin_memory().numpy().view(np.uint32) for c in cols]
+    c2 = R.Context(local)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    sm = torch.zeros(2, dtype=torch.int64, device=dev)
+
+    def step():
+        c2.load_columns(host)
+        c2.scan_aggregate_async(terms, 3, 1, cnt.data_ptr(), sm.data_ptr(), 0)
+        return cnt.cpu(), sm.cpu()
+    step()
+    reps = 3
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        step()
+    e_s = (time.perf_counter() - t0) / reps
+    c2.close()
+    return {"value": round(bytes_step * world / e_s / 1e9, 3), "unit": "GB/s",
+            "h2d_bytes_per_step": int(bytes_step), "d2h_bytes_per_step": 24,
+            "ms_per_step": round(e_s * 1e3, 2), "api": "rts_load_columns + rts_scan_aggregate_async"}
 
 
 SERVE_KINDS = ["uniform", "uniform", "zipf1.3", "zipf1.3"]
@@ -562,6 +674,10 @@ def run_reference(args):
         return
     from rtscan_b200 import datagen as D
     wl = args.workload
+    if wl == "q6":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no aggregate step (it stops at "
+                          "the bitmap); the q6 line's cpu_baseline times a numpy port"}), flush=True)
+        return
     kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, BATCH_KINDS)
     cols = cpu_sample_columns(kinds, REF_N)
     smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols]
@@ -603,7 +719,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "single", "multi"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "single", "multi", "q6"])
     ap.add_argument("--nrows", type=int, default=100_000_000)
     ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")

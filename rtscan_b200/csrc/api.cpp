@@ -70,6 +70,7 @@ void release_table(rts_ctx *ctx) {
   ctx->bindex.clear();
   if (ctx->owned) cudaFree(ctx->owned);
   ctx->owned = nullptr;
+  ctx->owned_bytes = 0;
   ctx->cols.clear();
   ctx->nrows = 0;
   for (uint32_t *p : ctx->scratch_bm) cudaFree(p);
@@ -269,13 +270,25 @@ rts_status rts_load_columns(rts_ctx *ctx, const uint32_t *const *host_cols, int3
     for (int c = 0; c < ncols; c++)
       if (!host_cols[c]) throw Error(RTS_ERR_ARG, "null column pointer");
     DeviceGuard g(ctx->device);
-    release_table(ctx);
-    // Pad each column to whole 1024-row tiles plus 16-byte alignment.
+    // Pad each column to whole 1024-row tiles plus 16-byte alignment; a
+    // table that fits the previous allocation reuses it.
     const uint64_t stride = (nrows + rts::kTileRows - 1) / rts::kTileRows * rts::kTileRows;
+    const size_t bytes = stride * ncols * sizeof(uint32_t);
     uint32_t *buf = nullptr;
-    if (cudaMalloc(&buf, stride * ncols * sizeof(uint32_t)) != cudaSuccess) {
-      cudaGetLastError();
-      throw Error(RTS_ERR_NOMEM, "device allocation of " + std::to_string(stride * ncols * 4) + " bytes failed");
+    const size_t kept = ctx->owned_bytes;
+    if (ctx->owned && kept >= bytes) {
+      buf = ctx->owned;
+      ctx->owned = nullptr;  // kept across release_table
+    }
+    release_table(ctx);
+    if (buf) {
+      ctx->owned_bytes = kept;
+    } else {
+      if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(RTS_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+      }
+      ctx->owned_bytes = bytes;
     }
     ctx->owned = buf;
     ctx->col_stride = stride;
@@ -314,6 +327,7 @@ rts_status rts_load_file(rts_ctx *ctx, const char *path, int32_t ncols, uint64_t
       throw Error(RTS_ERR_NOMEM, "device allocation failed");
     }
     ctx->owned = buf;
+    ctx->owned_bytes = stride * ncols * sizeof(uint32_t);
     ctx->col_stride = stride;
     const size_t chunk = 1u << 24;  // values per staging copy
     uint32_t *stage = nullptr;

@@ -122,6 +122,7 @@ struct rts_ctx {
   uint64_t nrows = 0;
   std::vector<const uint32_t *> cols;
   uint32_t *owned = nullptr;  // one allocation backing owned columns
+  size_t owned_bytes = 0;     // its size
   uint64_t col_stride = 0;    // values between owned columns
   std::vector<std::unique_ptr<rts::GpuBinDex>> bindex;
   // scratch for the separate-pass path and the BinDex planner
