@@ -492,6 +492,9 @@ def run(args):
         line["batch_config"]["source"] = "autotuned" if tuned else "default"
     line.update(extra)
 
+    if args.bindex_io and rank == 0:
+        line["bindex_io"] = bindex_io_leg(torch, R, dev, args.bindex_io)
+
     if wl == "batched" and args.pass_sweep:
         line["pass_sweep"] = pass_sweep(torch, R, D, dev, rank, args.pass_sweep)
 
@@ -529,6 +532,34 @@ def run(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def bindex_io_leg(torch, R, dev, n, K=128):
+    """BinDex of one n-row zipf 1.3 column: build on the device vs save to a
+    file and load it back (the load checks checksums and the sorted order
+    against the column)."""
+    col = gpu_column(torch, "zipf1.3", n, 99, dev)
+    c = R.Context(dev.index or 0)
+    c.attach_columns([col.data_ptr()], n)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    c.build_bindex(0, K)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "col0.bdx")
+        t0 = time.perf_counter()
+        c.save_bindex(0, path)
+        save_s = time.perf_counter() - t0
+        size = os.path.getsize(path)
+        c.drop_bindex(0)
+        t0 = time.perf_counter()
+        c.load_bindex(0, path)
+        load_s = time.perf_counter() - t0
+    c.close()
+    return {"rows": n, "K": K, "file_MB": round(size / 1e6, 1), "build_ms": round(build_s * 1e3, 1),
+            "save_ms": round(save_s * 1e3, 1), "load_ms": round(load_s * 1e3, 1),
+            "load_GB_s": round(size / load_s / 1e9, 2)}
 
 
 def q6_legs(torch, R, ctx, terms, n, out, cnt, s, timed, fused_ms):
@@ -727,6 +758,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the one-query-per-launch comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-scan leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch launch shape")
+    ap.add_argument("--bindex-io", type=int, default=0, metavar="ROWS",
+                    help="also time BinDex build vs save and load for a ROWS-row column (off by default)")
     ap.add_argument("--pass-sweep", type=int, default=0, metavar="ROWS",
                     help="also time one pass of 1..512 queries over a ROWS-row table (off by default)")
     ap.add_argument("--serve-rows", type=int, default=1 << 28)

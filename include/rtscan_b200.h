@@ -207,6 +207,17 @@ RTS_API rts_status rts_bindex_filter_vector(rts_ctx *ctx, int32_t column, int32_
 RTS_API rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms,
                                          uint32_t *dev_bitmap, uint64_t *dev_count, void *stream);
 
+/* Save a column's BinDex to a file and load it back into a context whose
+ * resident column is the same (no reference counterpart: the reference
+ * rebuilds every index at start-up, bindex_cuda.cpp:1769-1781).  The file
+ * carries a versioned header, checksums of every array (verified on load)
+ * and the index's K and row count; loading also checks the sorted order
+ * against the resident column and fails with RTS_ERR_PARSE on any mismatch.
+ * rts_bindex_file_info reads only the header (no GPU needed). */
+RTS_API rts_status rts_save_bindex(rts_ctx *ctx, int32_t column, const char *path);
+RTS_API rts_status rts_load_bindex(rts_ctx *ctx, int32_t column, const char *path);
+RTS_API rts_status rts_bindex_file_info(const char *path, int32_t *K, uint64_t *nrows);
+
 /* ---- batched scans -------------------------------------------------------- */
 
 /* Many queries in one pass (no reference counterpart; the reference runs one

@@ -118,6 +118,10 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_save_bindex", ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_char_p]),
+    ("rts_load_bindex", ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_char_p]),
+    ("rts_bindex_file_info", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.POINTER(ctypes.c_uint64)]),
     ("rts_bitmap_rows_async", ctypes.c_int32, [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P, _P]),
     ("rts_bitmap_sum_async", ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P]),
     ("rts_scan_aggregate_async", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P,
@@ -166,6 +170,14 @@ def _check(rc: int, ctx=None):
     if rc != 0:
         msg = lib().rts_last_error(ctx)
         raise RtsError(rc, msg.decode() if msg else "")
+
+
+def bindex_file_info(path: str):
+    """(K, nrows) from a saved BinDex file's header; raises on a bad file."""
+    k = ctypes.c_int32()
+    n = ctypes.c_uint64()
+    _check(lib().rts_bindex_file_info(path.encode(), ctypes.byref(k), ctypes.byref(n)))
+    return k.value, n.value
 
 
 def version() -> str:
@@ -428,6 +440,13 @@ class Context:
     def scan_async(self, terms, bitmap_ptr: int, count_ptr: int, stream: int = 0) -> None:
         arr, n = make_terms(terms)
         self._c(lib().rts_scan_async(self._h, arr, n, bitmap_ptr, count_ptr, stream))
+
+    def save_bindex(self, column: int, path: str) -> None:
+        self._c(lib().rts_save_bindex(self._h, column, path.encode()))
+
+    def load_bindex(self, column: int, path: str) -> None:
+        """Load a saved BinDex for `column` (checked against the resident column)."""
+        self._c(lib().rts_load_bindex(self._h, column, path.encode()))
 
     def bitmap_rows_async(self, bitmap_ptr: int, nrows: int, rows_ptr: int, capacity: int, count_ptr: int,
                           stream: int = 0) -> None:

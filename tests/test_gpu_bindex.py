@@ -105,3 +105,58 @@ def test_blocking_scan_uses_index(ctx):
     bm, cnt = ctx.scan(q)
     want, wcnt = expect(cols, q)
     assert cnt == wcnt and np.array_equal(bm, want)
+
+
+@pytest.mark.parametrize("K", [4, 128])
+def test_saved_index_loads_and_answers_the_same(ctx, tmp_path, K):
+    n = 700_001
+    cols = [D.zipf(n, 31, 1.3), D.uniform(n, 32), D.normal(n, 33)]
+    ctx.load_columns(cols)
+    for c in range(3):
+        ctx.build_bindex(c, K)
+        ctx.save_bindex(c, str(tmp_path / f"c{c}.bdx"))
+    assert R.bindex_file_info(str(tmp_path / "c0.bdx")) == (K, n)
+    rng = np.random.default_rng(4)
+    qs = D.batch_queries(cols, 30, seed=5) + [[(0, 0, 3)], [(2, 1 << 31, 0xFFFFFFFF), (1, 7, 1 << 30)]]
+    before = [bindex_scan(ctx, q) for q in qs]
+    fvs = [ctx.bindex_filter_vector(0, k) for k in (0, K // 2, K - 2)]
+    areas = ctx.bindex_areas(1, K)
+    # a fresh table from the same columns, indexes from the files
+    ctx.load_columns(cols)
+    for c in range(3):
+        ctx.load_bindex(c, str(tmp_path / f"c{c}.bdx"))
+    for q, (bm, cnt) in zip(qs, before):
+        got, gcnt = bindex_scan(ctx, q)
+        want, wcnt = expect(cols, q)
+        assert gcnt == cnt == wcnt and np.array_equal(got, bm) and np.array_equal(got, want), q
+    for k, fv in zip((0, K // 2, K - 2), fvs):
+        assert np.array_equal(ctx.bindex_filter_vector(0, k), fv)
+    s2, r2 = ctx.bindex_areas(1, K)
+    assert np.array_equal(s2, areas[0]) and np.array_equal(r2, areas[1])
+
+
+def test_loading_rejects_other_columns_and_damage(ctx, tmp_path):
+    n = 200_003
+    a, b = D.uniform(n, 41), D.uniform(n, 42)
+    ctx.load_columns([a, b])
+    ctx.build_bindex(0, 16)
+    f = tmp_path / "a.bdx"
+    ctx.save_bindex(0, str(f))
+    with pytest.raises(R.RtsError) as e:        # the index of column 0 against column 1
+        ctx.load_bindex(1, str(f))
+    assert e.value.code == -5
+    raw = bytearray(f.read_bytes())
+    raw[len(raw) // 2] ^= 0x10                   # one bit in the payload
+    bad = tmp_path / "bad.bdx"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(R.RtsError) as e:
+        ctx.load_bindex(0, str(bad))
+    assert e.value.code == -5
+    short = tmp_path / "short.bdx"
+    short.write_bytes(f.read_bytes()[:-4096])
+    with pytest.raises(R.RtsError) as e:
+        ctx.load_bindex(0, str(short))
+    assert e.value.code == -5
+    ctx.load_columns([a[:-5]])                   # a table of another size
+    with pytest.raises(R.RtsError):
+        ctx.load_bindex(0, str(f))
