@@ -324,6 +324,21 @@ RTS_API rts_status rts_server_stop(rts_server *srv);
 RTS_API rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets,
                                      int32_t nqueries, const double *arrival_s, double *latency_ms);
 
+/* ---- rank encoding (remap.cpp) ---------------------------------------------- */
+/* Replace every resident column by codes: row r's value becomes
+ * encode_min + rank(r) * step, rank(r) its position in the column's stable
+ * sorted order (ties by row id) and step = max(1, (encode_max - encode_min) /
+ * nrows); the range must hold a code per row.  Indexes are dropped; borrowed
+ * columns are not modified (the codes live in the context).  The
+ * reference's normalEncode (remap.cpp:110-209) spreads the rows of one value
+ * with rand(); this encoding is deterministic and order-preserving. */
+RTS_API rts_status rts_encode_table(rts_ctx *ctx, uint32_t encode_min, uint32_t encode_max);
+/* Rewrite terms on the original values into terms on the codes (encodeQuery,
+ * remap.cpp:242-270, exact for every bound): out[i] selects on the encoded
+ * table exactly the rows terms[i] selects on the original one; a term that
+ * no value satisfies becomes the empty term lo = 1, hi = 0. */
+RTS_API rts_status rts_encode_terms(rts_ctx *ctx, const rts_term *terms, int32_t nterms, rts_term *out);
+
 /* ---- after the scan: row ids and aggregates --------------------------------- */
 /* No reference counterpart: the reference stops at the bitmap and its hit
  * count, and its query files name the step that follows in a query engine

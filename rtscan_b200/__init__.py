@@ -118,6 +118,8 @@ _SIGS = [
                                              _P]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
+    ("rts_encode_table", ctypes.c_int32, [_P, ctypes.c_uint32, ctypes.c_uint32]),
+    ("rts_encode_terms", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, _TERMP]),
     ("rts_save_bindex", ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_char_p]),
     ("rts_load_bindex", ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_char_p]),
     ("rts_bindex_file_info", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32),
@@ -440,6 +442,18 @@ class Context:
     def scan_async(self, terms, bitmap_ptr: int, count_ptr: int, stream: int = 0) -> None:
         arr, n = make_terms(terms)
         self._c(lib().rts_scan_async(self._h, arr, n, bitmap_ptr, count_ptr, stream))
+
+    def encode_table(self, encode_min: int = 0, encode_max: int = 0) -> None:
+        """Rank-encode the resident table (codes in [encode_min, encode_max),
+        default [0, nrows))."""
+        self._c(lib().rts_encode_table(self._h, encode_min, encode_max or self.nrows))
+
+    def encode_terms(self, terms):
+        """Terms on the original values -> terms on the codes."""
+        arr, n = make_terms(terms)
+        out = (Term * max(1, n))()
+        self._c(lib().rts_encode_terms(self._h, arr, n, out))
+        return [(t.column, t.lo, t.hi) for t in out[:n]]
 
     def save_bindex(self, column: int, path: str) -> None:
         self._c(lib().rts_save_bindex(self._h, column, path.encode()))

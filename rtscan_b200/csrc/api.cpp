@@ -68,6 +68,7 @@ void need_table(rts_ctx *ctx) {
 
 void release_table(rts_ctx *ctx) {
   ctx->bindex.clear();
+  ctx->encode.reset();
   if (ctx->owned) cudaFree(ctx->owned);
   ctx->owned = nullptr;
   ctx->owned_bytes = 0;

@@ -9,13 +9,18 @@
 // self-check compares the chosen plan with the plain fused scan on the GPU
 // (the reference re-runs its scalar filter on the host, bindex_cuda.cpp:
 // 1948-1983); `-m` picks the plan (auto | scan | bindex | batch); `-o`
-// writes each result bitmap to <prefix>.<query>.bin.
+// writes each result bitmap to <prefix>.<query>.bin; `-e` rank-encodes the
+// table first and rewrites every query (the reference's ENCODE=1 build of
+// its RT driver, rtscan.cpp:1020-1024,1069-1072); `-I <prefix>` loads each
+// column's index from <prefix>.<column>.bdx when present and saves it there
+// after building it otherwise.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
 #include <vector>
@@ -43,15 +48,18 @@ static uint64_t popcount_host(const std::vector<uint32_t> &a, const std::vector<
 
 int main(int argc, char **argv) {
   const char *data = nullptr, *cmd_path = "test/scan_cmd.txt", *out_prefix = nullptr, *mode = "auto";
+  const char *index_prefix = nullptr;
+  bool encode = false;
   int ncols = 1, K = 128, device = 0;
   uint64_t nrows = 0;
   bool check = true;
   int opt;
-  while ((opt = getopt(argc, argv, "hf:b:p:n:K:m:o:d:x")) != -1) {
+  while ((opt = getopt(argc, argv, "hf:b:p:n:K:m:o:d:xeI:")) != -1) {
     switch (opt) {
       case 'h':
         printf("Usage: %s -f <column-file> -b <ncols> -p <scan-cmd-file> [-n <rows>] [-K <areas>]\n"
-               "          [-m auto|scan|bindex|batch] [-o <bitmap-prefix>] [-d <device>] [-x (no check)]\n",
+               "          [-m auto|scan|bindex|batch] [-o <bitmap-prefix>] [-d <device>] [-x (no check)]\n"
+               "          [-e (rank-encode the table)] [-I <index-file-prefix>]\n",
                argv[0]);
         return 0;
       case 'f': data = optarg; break;
@@ -63,6 +71,8 @@ int main(int argc, char **argv) {
       case 'o': out_prefix = optarg; break;
       case 'd': device = atoi(optarg); break;
       case 'x': check = false; break;
+      case 'e': encode = true; break;
+      case 'I': index_prefix = optarg; break;
       default: fprintf(stderr, "Error: unknown option %c\n", (char)opt); return 2;
     }
   }
@@ -75,11 +85,23 @@ int main(int argc, char **argv) {
   if (rts_load_file(ctx, data, ncols, nrows) != RTS_OK) return die(ctx, "load");
   const uint64_t n = rts_nrows(ctx), words = rts_bitmap_words(n);
   printf("N = %llu\n", (unsigned long long)n);
+  if (encode) {
+    const double te = now_ms();
+    if (rts_encode_table(ctx, 0, (uint32_t)std::min<uint64_t>(n, 0xFFFFFFFFull)) != RTS_OK) return die(ctx, "encode");
+    printf("[Time] Encode Time: %.3f ms\n", now_ms() - te);
+  }
   const bool want_index = !strcmp(mode, "auto") || !strcmp(mode, "bindex");
   double t0 = now_ms();
   if (want_index)
-    for (int c = 0; c < ncols; c++)
+    for (int c = 0; c < ncols; c++) {
+      const std::string fn = index_prefix ? std::string(index_prefix) + "." + std::to_string(c) + ".bdx" : "";
+      if (index_prefix && access(fn.c_str(), R_OK) == 0) {
+        if (rts_load_bindex(ctx, c, fn.c_str()) != RTS_OK) return die(ctx, "load bindex");
+        continue;
+      }
       if (rts_build_bindex(ctx, c, K) != RTS_OK) return die(ctx, "build bindex");
+      if (index_prefix && rts_save_bindex(ctx, c, fn.c_str()) != RTS_OK) return die(ctx, "save bindex");
+    }
   printf("[Time] Index Build Time: %.3f ms\n", now_ms() - t0);
 
   FILE *fp = fopen(cmd_path, "rb");
@@ -109,6 +131,11 @@ int main(int argc, char **argv) {
     const rts_term *terms;
     int32_t nt, empty;
     rts_qset_query(qs, q, &terms, &nt, &empty);
+    std::vector<rts_term> coded(nt);
+    if (encode && nt > 0) {
+      if (rts_encode_terms(ctx, terms, nt, coded.data()) != RTS_OK) return die(ctx, "encode query");
+      terms = coded.data();
+    }
     for (int c = 0; c < ncols; c++) {
       int32_t op;
       uint32_t t1, t2;

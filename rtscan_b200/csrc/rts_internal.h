@@ -92,6 +92,16 @@ std::unique_ptr<GpuBinDex> build_bindex(const uint32_t *col, uint64_t n, int K, 
 void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out, unsigned long long *count,
                   cudaStream_t s);
 
+// Rank encoding of the resident table (encode.cu): per column the sorted
+// original values (the value -> code map), and the code of rank r is
+// min + r * step.
+struct EncodeMap {
+  uint64_t n = 0;
+  uint32_t min = 0, step = 1;
+  std::vector<uint32_t *> sval;
+  ~EncodeMap();
+};
+
 // A 256-byte device buffer owned by the context (blocking-call counts).
 unsigned long long *small_device_buffer(rts_ctx *ctx);
 
@@ -137,6 +147,7 @@ struct rts_ctx {
   rts::BatchScratch *batch = nullptr;
   rts::HostBatchBuffers *host_batch = nullptr;
   rts::BatchConfig batch_cfg;
+  std::unique_ptr<rts::EncodeMap> encode;  // set by rts_encode_table
   std::atomic<uint64_t> launches{0};
   std::string err;
   ~rts_ctx();
