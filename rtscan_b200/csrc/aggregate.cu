@@ -350,6 +350,7 @@ extern "C" {
 
 rts_status rts_bitmap_rows_async(rts_ctx *ctx, const uint32_t *dev_bitmap, uint64_t nrows, uint32_t *dev_rows,
                                  uint64_t capacity, uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_bitmap_rows_async");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!dev_bitmap || !dev_count || (capacity && !dev_rows)) throw rts::Error(RTS_ERR_ARG, "null argument");
@@ -382,6 +383,7 @@ rts_status rts_bitmap_rows_async(rts_ctx *ctx, const uint32_t *dev_bitmap, uint6
 
 rts_status rts_bitmap_sum_async(rts_ctx *ctx, const uint32_t *dev_bitmap, int32_t col_a, int32_t col_b,
                                 uint64_t *dev_sum, void *stream) {
+  rts::Range nvtx_range_("rts_bitmap_sum_async");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!dev_bitmap || !dev_sum) throw rts::Error(RTS_ERR_ARG, "null argument");
@@ -407,6 +409,7 @@ rts_status rts_bitmap_sum_async(rts_ctx *ctx, const uint32_t *dev_bitmap, int32_
 
 rts_status rts_scan_aggregate_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, int32_t col_a,
                                     int32_t col_b, uint64_t *dev_count, uint64_t *dev_sum, void *stream) {
+  rts::Range nvtx_range_("rts_scan_aggregate_async");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (nterms < 0 || (nterms > 0 && !terms)) throw rts::Error(RTS_ERR_ARG, "bad terms");

@@ -265,6 +265,7 @@ void rts_close(rts_ctx *ctx) {
 }
 
 rts_status rts_load_columns(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols, uint64_t nrows) {
+  rts::Range nvtx_range_("rts_load_columns");
   return guarded(ctx, [&]() -> rts_status {
     need_ctx(ctx);
     if (ncols < 1 || nrows == 0 || !host_cols) throw Error(RTS_ERR_ARG, "need ncols >= 1, nrows >= 1 and columns");
@@ -306,6 +307,7 @@ rts_status rts_load_columns(rts_ctx *ctx, const uint32_t *const *host_cols, int3
 }
 
 rts_status rts_load_file(rts_ctx *ctx, const char *path, int32_t ncols, uint64_t nrows) {
+  rts::Range nvtx_range_("rts_load_file");
   return guarded(ctx, [&]() -> rts_status {
     need_ctx(ctx);
     if (!path || ncols < 1) throw Error(RTS_ERR_ARG, "need a path and ncols >= 1");
@@ -384,6 +386,7 @@ uint64_t rts_kernel_launches(const rts_ctx *ctx) { return ctx ? ctx->launches.lo
 
 rts_status rts_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
                           uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_scan_async");
   return guarded(ctx, [&]() -> rts_status {
     need_table(ctx);
     if (!dev_bitmap) throw Error(RTS_ERR_ARG, "null result bitmap");
@@ -396,6 +399,7 @@ rts_status rts_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, u
 
 rts_status rts_scan_separate_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
                                    uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_scan_separate_async");
   return guarded(ctx, [&]() -> rts_status {
     need_table(ctx);
     if (!dev_bitmap) throw Error(RTS_ERR_ARG, "null result bitmap");
@@ -434,6 +438,7 @@ rts_status rts_scan_separate_async(rts_ctx *ctx, const rts_term *terms, int32_t 
 }
 
 rts_status rts_scan(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *host_bitmap, uint64_t *count) {
+  rts::Range nvtx_range_("rts_scan");
   return guarded(ctx, [&]() -> rts_status {
     need_table(ctx);
     if (!count) throw Error(RTS_ERR_ARG, "null count pointer");
@@ -491,6 +496,7 @@ rts_status rts_bitmap_count_async(rts_ctx *ctx, const uint32_t *bitmap, uint64_t
 
 rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
                                uint32_t *dev_bitmaps, uint64_t stride_words, uint64_t *dev_counts, void *stream) {
+  rts::Range nvtx_range_("rts_scan_each_async");
   return guarded(ctx, [&]() -> rts_status {
     need_table(ctx);
     if (nq < 0 || (nq > 0 && (!offsets || !dev_bitmaps))) throw Error(RTS_ERR_ARG, "bad batch arguments");

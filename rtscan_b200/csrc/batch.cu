@@ -966,6 +966,7 @@ static void ensure(T *&p, size_t &cap, size_t count) {
 extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
                                           uint64_t nrows, const rts_term *terms, const int32_t *offsets, int32_t nq,
                                           uint32_t *host_bitmaps, uint64_t stride_words, uint64_t *host_counts) {
+  rts::Range nvtx_range_("rts_scan_batch_host");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!host_cols || ncols < 1 || nrows == 0) throw rts::Error(RTS_ERR_ARG, "need host columns");
@@ -1075,6 +1076,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
 extern "C" rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
                                            uint32_t *dev_bitmaps, uint64_t stride_words, uint64_t *dev_counts,
                                            void *stream) {
+  rts::Range nvtx_range_("rts_scan_batch_async");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");

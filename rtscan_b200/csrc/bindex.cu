@@ -639,6 +639,7 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
 extern "C" {
 
 rts_status rts_build_bindex(rts_ctx *ctx, int32_t column, int32_t K) {
+  rts::Range nvtx_range_("rts_build_bindex");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");
@@ -701,6 +702,7 @@ rts_status rts_bindex_filter_vector(rts_ctx *ctx, int32_t column, int32_t k, uin
 
 rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
                                  uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_bindex_scan_async");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");

@@ -162,6 +162,7 @@ rts_status fail(rts_ctx *ctx, rts_status code, const char *what) {
 extern "C" {
 
 rts_status rts_save_bindex(rts_ctx *ctx, int32_t column, const char *path) {
+  rts::Range nvtx_range_("rts_save_bindex");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!path) throw rts::Error(RTS_ERR_ARG, "null path");
@@ -230,6 +231,7 @@ rts_status rts_bindex_file_info(const char *path, int32_t *K, uint64_t *nrows) {
 }
 
 rts_status rts_load_bindex(rts_ctx *ctx, int32_t column, const char *path) {
+  rts::Range nvtx_range_("rts_load_bindex");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!path) throw rts::Error(RTS_ERR_ARG, "null path");

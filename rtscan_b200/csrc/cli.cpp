@@ -13,7 +13,11 @@
 // table first and rewrites every query (the reference's ENCODE=1 build of
 // its RT driver, rtscan.cpp:1020-1024,1069-1072); `-I <prefix>` loads each
 // column's index from <prefix>.<column>.bdx when present and saves it there
-// after building it otherwise.
+// after building it otherwise; `-q <n>` answers the first n queries of the
+// file, or with `-y 0` generates n queries instead (the reference RT
+// driver's flags, rtscan.cpp:939-958,798-865): `-g 1` (default) range
+// queries `lt (i+1)*span` on every column, `-g 0` point queries
+// `eq (i+1)*span`, span = (2^32 - 1) / (n + 1).
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -49,17 +53,19 @@ static uint64_t popcount_host(const std::vector<uint32_t> &a, const std::vector<
 int main(int argc, char **argv) {
   const char *data = nullptr, *cmd_path = "test/scan_cmd.txt", *out_prefix = nullptr, *mode = "auto";
   const char *index_prefix = nullptr;
-  bool encode = false;
+  bool encode = false, read_queries = true, range_queries = true;
+  int max_queries = -1;
   int ncols = 1, K = 128, device = 0;
   uint64_t nrows = 0;
   bool check = true;
   int opt;
-  while ((opt = getopt(argc, argv, "hf:b:p:n:K:m:o:d:xeI:")) != -1) {
+  while ((opt = getopt(argc, argv, "hf:b:p:n:K:m:o:d:xeI:q:y:g:")) != -1) {
     switch (opt) {
       case 'h':
         printf("Usage: %s -f <column-file> -b <ncols> -p <scan-cmd-file> [-n <rows>] [-K <areas>]\n"
                "          [-m auto|scan|bindex|batch] [-o <bitmap-prefix>] [-d <device>] [-x (no check)]\n"
-               "          [-e (rank-encode the table)] [-I <index-file-prefix>]\n",
+               "          [-e (rank-encode the table)] [-I <index-file-prefix>]\n"
+               "          [-q <queries>] [-y 0 (generate the queries)] [-g 1|0 (range|point queries)]\n",
                argv[0]);
         return 0;
       case 'f': data = optarg; break;
@@ -73,6 +79,9 @@ int main(int argc, char **argv) {
       case 'x': check = false; break;
       case 'e': encode = true; break;
       case 'I': index_prefix = optarg; break;
+      case 'q': max_queries = atoi(optarg); break;
+      case 'y': read_queries = atoi(optarg) != 0; break;
+      case 'g': range_queries = atoi(optarg) != 0; break;
       default: fprintf(stderr, "Error: unknown option %c\n", (char)opt); return 2;
     }
   }
@@ -82,7 +91,11 @@ int main(int argc, char **argv) {
   }
   rts_ctx *ctx = nullptr;
   if (rts_open(device, &ctx) != RTS_OK) return die(nullptr, "open");
+  size_t free0 = 0, free1 = 0, total = 0;
+  cudaMemGetInfo(&free0, &total);
   if (rts_load_file(ctx, data, ncols, nrows) != RTS_OK) return die(ctx, "load");
+  cudaMemGetInfo(&free1, &total);
+  printf("[Mem] columns: %.1f MB used\n", (double)(free0 - free1) / 1e6);
   const uint64_t n = rts_nrows(ctx), words = rts_bitmap_words(n);
   printf("N = %llu\n", (unsigned long long)n);
   if (encode) {
@@ -103,20 +116,37 @@ int main(int argc, char **argv) {
       if (index_prefix && rts_save_bindex(ctx, c, fn.c_str()) != RTS_OK) return die(ctx, "save bindex");
     }
   printf("[Time] Index Build Time: %.3f ms\n", now_ms() - t0);
-
-  FILE *fp = fopen(cmd_path, "rb");
-  if (!fp) {
-    fprintf(stderr, "Fail to open scan_cmd file %s\n", cmd_path);
-    return 1;
+  {
+    size_t free2 = 0;
+    cudaMemGetInfo(&free2, &total);
+    printf("[Mem] indexes: %.1f MB used\n", (double)(free1 - free2) / 1e6);
   }
+
   std::string text;
-  char buf[1 << 16];
-  size_t r;
-  while ((r = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, r);
-  fclose(fp);
+  if (read_queries) {
+    FILE *fp = fopen(cmd_path, "rb");
+    if (!fp) {
+      fprintf(stderr, "Fail to open scan_cmd file %s\n", cmd_path);
+      return 1;
+    }
+    char buf[1 << 16];
+    size_t r;
+    while ((r = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, r);
+    fclose(fp);
+  } else {
+    if (max_queries < 1) {
+      fprintf(stderr, "-y 0 needs -q <queries>\n");
+      return 2;
+    }
+    const uint32_t span = 0xFFFFFFFFu / (uint32_t)(max_queries + 1);
+    for (int i = 0; i < max_queries; i++)
+      for (int c = 0; c < ncols; c++)
+        text += std::string(range_queries ? "lt " : "eq ") + std::to_string((uint64_t)(i + 1) * span) + "\n";
+    text += "exit\n";
+  }
   rts_qset *qs = nullptr;
   if (rts_parse_scan_cmd(text.data(), text.size(), ncols, &qs) != RTS_OK) return die(nullptr, "scan_cmd");
-  const int nq = rts_qset_size(qs);
+  const int nq = max_queries >= 0 ? std::min(max_queries, (int)rts_qset_size(qs)) : (int)rts_qset_size(qs);
 
   uint32_t *d_bm = nullptr, *d_chk = nullptr;
   uint64_t *d_cnt = nullptr;

@@ -104,6 +104,7 @@ EncodeMap::~EncodeMap() {
 extern "C" {
 
 rts_status rts_encode_table(rts_ctx *ctx, uint32_t encode_min, uint32_t encode_max) {
+  rts::Range nvtx_range_("rts_encode_table");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");
@@ -163,6 +164,7 @@ rts_status rts_encode_table(rts_ctx *ctx, uint32_t encode_min, uint32_t encode_m
 }
 
 rts_status rts_encode_terms(rts_ctx *ctx, const rts_term *terms, int32_t nterms, rts_term *out) {
+  rts::Range nvtx_range_("rts_encode_terms");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   try {
     if (!ctx->encode) throw rts::Error(RTS_ERR_STATE, "table is not encoded (rts_encode_table)");

@@ -40,6 +40,7 @@ extern "C" {
 
 rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
                              uint32_t *dev_bitmaps, uint64_t stride_words, uint64_t *dev_counts, rts_prepared **out) {
+  rts::Range nvtx_range_("rts_batch_prepare");
   if (!ctx || !out) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
   *out = nullptr;
   if (ctx->cols.empty()) return fail(ctx, RTS_ERR_STATE, "no columns loaded");
@@ -98,6 +99,7 @@ rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t 
 }
 
 rts_status rts_batch_launch(rts_prepared *p, void *stream) {
+  rts::Range nvtx_range_("rts_batch_launch");
   if (!p) return rts::set_thread_error(RTS_ERR_ARG, "null prepared batch");
   cudaError_t e = cudaGraphLaunch(p->exec, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(p->ctx, RTS_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));

@@ -58,6 +58,7 @@ bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 extern "C" rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev_cols, int32_t ncols, uint64_t nrows,
                                                       const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
                                                       uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_scan_separate_noalloc_async");
   using rts::set_thread_error;
   if (nrows > RTS_NOALLOC_MAX_ROWS)
     return set_thread_error(RTS_ERR_ARG, "nrows " + std::to_string(nrows) +

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <atomic>
@@ -33,6 +34,15 @@ struct Error : std::runtime_error {
     if (e_ != cudaSuccess)                                                                  \
       throw ::rts::Error(RTS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// NVTX range for the lifetime of the object: library calls and server steps
+// show up by name in nsys/ncu timelines (no cost without an attached tool).
+struct Range {
+  explicit Range(const char *name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range &) = delete;
+  Range &operator=(const Range &) = delete;
+};
 
 // Record `msg` as the calling thread's last error (rts_last_error(NULL)).
 rts_status set_thread_error(rts_status code, const std::string &msg);

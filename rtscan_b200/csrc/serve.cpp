@@ -181,6 +181,7 @@ struct rts_server {
   }
 
   void step() {
+    rts::Range nvtx_range_("rts_server_step");
     std::vector<int> active;
     for (size_t i = 0; i < slots.size(); i++)
       if (slots[i].state == ACTIVE) active.push_back((int)i);
@@ -535,6 +536,7 @@ rts_status rts_server_stop(rts_server *srv) {
 // the queue was full).  Blocks until every request is done.
 rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets, int32_t nq,
                              const double *arrival_s, double *latency_ms) {
+  rts::Range nvtx_range_("rts_server_replay");
   if (!srv || nq < 0 || (nq > 0 && (!offsets || !arrival_s || !latency_ms)))
     return fail(srv, RTS_ERR_ARG, "bad replay arguments");
   std::unordered_map<uint64_t, int> index_of;  // ticket -> query, filled by the producer

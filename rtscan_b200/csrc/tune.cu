@@ -119,6 +119,7 @@ rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg) {
 
 rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,
                               const char *cache_path, rts_batch_config *best_out) {
+  rts::Range nvtx_range_("rts_autotune_batch");
   if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
   if (ctx->cols.empty()) return rts::set_thread_error(RTS_ERR_STATE, "no columns loaded");
   if (nq < 1 || !offsets) return rts::set_thread_error(RTS_ERR_ARG, "need at least one query");

@@ -59,3 +59,22 @@ def test_cli_index_files(table):
     second = run_cli(["-f", data, "-b", "3", "-p", cmd, "-m", "bindex", "-I", prefix])  # loads the files
     for out in (first, second):
         assert [int(x) for x in re.findall(r"\[RESULT\] query \d+ count (\d+)", out)] == want
+
+
+def test_cli_query_count_and_generated_queries(table):
+    d, data, cmd, want = table
+    out = run_cli(["-f", data, "-b", "3", "-p", cmd, "-m", "scan", "-q", "5"])
+    assert [int(x) for x in re.findall(r"\[RESULT\] query \d+ count (\d+)", out)] == want[:5]
+    assert "[Mem] columns:" in out
+    cols = D.read_columns(data, 3, 400_009)
+    for g, op in ((1, "lt"), (0, "eq")):
+        out = run_cli(["-f", data, "-b", "3", "-y", "0", "-q", "6", "-g", str(g), "-m", "batch"])
+        span = 0xFFFFFFFF // 7
+        exp = []
+        for i in range(6):
+            t = (i + 1) * span
+            hit = np.ones(len(cols[0]), bool)
+            for c in cols:
+                hit &= (c < t) if op == "lt" else (c == t)
+            exp.append(int(hit.sum()))
+        assert [int(x) for x in re.findall(r"\[RESULT\] query \d+ count (\d+)", out)] == exp
