@@ -191,3 +191,43 @@ def test_reference_operator_lines(ctx):
         want = O.raw_scan_entry(cols, ref[i])
         assert cnt == O.popcount(want, n)
         assert np.array_equal(got, O.mask_tail(want, n))
+
+
+def test_all_equal_column(ctx):
+    n = 70_000
+    col = np.full(n, 123456, np.uint32)
+    ctx.load_columns([col])
+    for lo, hi in [(123456, 123456), (0, 123455), (123457, 0xFFFFFFFF), (0, 0xFFFFFFFF), (123456, 0xFFFFFFFF)]:
+        check(ctx, [col], [(0, lo, hi)])
+
+
+def test_load_file_and_its_failures(ctx, tmp_path):
+    n = 10_007
+    cols = [D.uniform(n, 61), D.uniform(n, 62, 100)]
+    f = tmp_path / "t.bin"
+    D.write_columns(str(f), cols)
+    ctx.load_file(str(f), 2)
+    assert ctx.nrows == n
+    check(ctx, cols, [(1, 10, 20), (0, 0, 1 << 31)])
+    short = tmp_path / "short.bin"
+    short.write_bytes(f.read_bytes()[:-4])
+    with pytest.raises(R.RtsError) as e:
+        ctx.load_file(str(short), 2, n)               # fewer bytes than 2 x n values
+    assert e.value.code == -4
+    with pytest.raises(R.RtsError) as e:
+        ctx.load_file(str(tmp_path / "none.bin"), 2)
+    assert e.value.code == -4
+    with pytest.raises(R.RtsError):
+        ctx.load_file(str(f), 0)
+
+
+def test_server_result_pool_too_large_is_refused(ctx):
+    n = 1 << 20
+    col = D.uniform(n, 63)
+    ctx.load_columns([col])
+    with pytest.raises(R.RtsError) as e:            # 2^24 slots x 128 KiB bitmaps: no such device memory
+        R.Server(ctx, max_active=1 << 24, segment_rows=1 << 16)
+    assert e.value.code == -3
+    with R.Server(ctx, max_active=4, segment_rows=1 << 16) as srv:   # the context still works
+        t = srv.submit([(0, 0, 1 << 31)])
+        assert srv.wait(t, 5000) == int((col <= (1 << 31)).sum())
