@@ -50,33 +50,28 @@ using V4Pos = typename std::conditional<(CMAX <= 4), uint32_t, uint16_t>::type;
 template <int CMAX, int GV>
 constexpr int kV4PosBytes = (V4Shape<GV>::kRows + V4Shape<GV>::kTiles) * CMAX * (int)sizeof(V4Pos<CMAX>);
 
-// Exchange the bits of a under mask M << S with the bits of b under M:
-// each result is one shift and one bitwise select.
+// Exchange the bits of a under mask M << S with the bits of b under M (a
+// delta swap: the XOR of the two bit sets applied to both; measured faster
+// here than two shift-and-select results).
 template <int S, uint32_t M>
 __device__ __forceinline__ void swap_bits(uint32_t &a, uint32_t &b) {
-  const uint32_t na = (a & ~(M << S)) | ((b << S) & (M << S));
-  const uint32_t nb = (b & ~M) | ((a >> S) & M);
-  a = na;
-  b = nb;
+  const uint32_t t = ((a >> S) ^ b) & M;
+  b ^= t;
+  a ^= t << S;
 }
 
 // 32x32 bit transpose in registers: on return bit j of x[i] is the input's
-// bit i of x[j].  Two byte-permute stages (16, 8) and three delta swaps.
+// bit i of x[j].  Each stage exchanges one bit of the row index with the
+// same bit of the column index, so the stages commute: three delta swaps
+// (1-, 2-, 4-bit blocks) and then two byte-permute stages (8-, 16-bit), the
+// order measured fastest.
 __device__ __forceinline__ void transpose32(uint32_t (&x)[32]) {
 #pragma unroll
-  for (int i = 0; i < 16; i++) {  // swap the off-diagonal 16x16 blocks
-    const uint32_t a = x[i], b = x[i + 16];
-    x[i] = __byte_perm(a, b, 0x5410);       // low halves: a.lo | b.lo << 16
-    x[i + 16] = __byte_perm(a, b, 0x7632);  // high halves: a.hi | b.hi << 16
-  }
+  for (int i = 0; i < 32; i += 2) swap_bits<1, 0x55555555u>(x[i], x[i + 1]);
 #pragma unroll
-  for (int base = 0; base < 32; base += 16) {
+  for (int base = 0; base < 32; base += 4) {
 #pragma unroll
-    for (int i = base; i < base + 8; i++) {  // 8x8 blocks: bytes 1<->0 and 3<->2
-      const uint32_t a = x[i], b = x[i + 8];
-      x[i] = __byte_perm(a, b, 0x6240);
-      x[i + 8] = __byte_perm(a, b, 0x7351);
-    }
+    for (int i = base; i < base + 2; i++) swap_bits<2, 0x33333333u>(x[i], x[i + 2]);
   }
 #pragma unroll
   for (int base = 0; base < 32; base += 8) {
@@ -84,12 +79,20 @@ __device__ __forceinline__ void transpose32(uint32_t (&x)[32]) {
     for (int i = base; i < base + 4; i++) swap_bits<4, 0x0F0F0F0Fu>(x[i], x[i + 4]);
   }
 #pragma unroll
-  for (int base = 0; base < 32; base += 4) {
+  for (int base = 0; base < 32; base += 16) {
 #pragma unroll
-    for (int i = base; i < base + 2; i++) swap_bits<2, 0x33333333u>(x[i], x[i + 2]);
+    for (int i = base; i < base + 8; i++) {
+      const uint32_t a = x[i], b = x[i + 8];
+      x[i] = __byte_perm(a, b, 0x6240);      // 8x8 blocks: bytes 1<->0 and 3<->2
+      x[i + 8] = __byte_perm(a, b, 0x7351);
+    }
   }
 #pragma unroll
-  for (int i = 0; i < 32; i += 2) swap_bits<1, 0x55555555u>(x[i], x[i + 1]);
+  for (int i = 0; i < 16; i++) {  // the off-diagonal 16x16 blocks
+    const uint32_t a = x[i], b = x[i + 16];
+    x[i] = __byte_perm(a, b, 0x5410);       // low halves: a.lo | b.lo << 16
+    x[i + 16] = __byte_perm(a, b, 0x7632);  // high halves: a.hi | b.hi << 16
+  }
 }
 
 template <int CMAX, int GV>
