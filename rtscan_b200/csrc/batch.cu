@@ -335,11 +335,8 @@ size_t smem_bytes(uint32_t blob_words) {
 
 template <int CMAX, int W>
 int blocks_per_sm(size_t smem) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(batch_kernel<CMAX, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> raised{0};
+  raise_smem_limit(batch_kernel<CMAX, W>, raised, 227 * 1024);
   int b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<CMAX, W>, W * 32, smem) != cudaSuccess ||
       b < 1)
@@ -366,11 +363,8 @@ size_t smem_bytes4(uint32_t blob_words) {
 
 template <int CMAX, int GV>
 void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(batch4_kernel<CMAX, GV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> raised{0};
+  raise_smem_limit(batch4_kernel<CMAX, GV>, raised, 227 * 1024);
   const size_t sm = smem_bytes4<CMAX, GV>(bp.blob_words);
   if (sm > 227 * 1024) throw Error(RTS_ERR_ARG, "batch pass exceeds shared memory");
   const uint64_t want = bp.nblocks - bp.block_begin;

@@ -44,6 +44,20 @@ struct Range {
   Range &operator=(const Range &) = delete;
 };
 
+// Raise `kernel`'s dynamic shared-memory limit to `bytes` on the current
+// device.  The attribute belongs to each device's context, so it is set once
+// per device (bit d of `done`), and calls from several threads at once only
+// set it twice.
+template <class K>
+void raise_smem_limit(K kernel, std::atomic<uint64_t> &done, int bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return;
+  RTS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 // Record `msg` as the calling thread's last error (rts_last_error(NULL)).
 rts_status set_thread_error(rts_status code, const std::string &msg);
 
@@ -120,11 +134,12 @@ struct BatchScratch;
 void destroy_batch(BatchScratch *b);
 struct HostBatchBuffers;
 void destroy_host_batch(HostBatchBuffers *b);
-// Launch shape of the batched kernel: warps per CTA (8 or 16), queries per
-// pass (<= 256) and the shared-memory bytes a pass may spend on its mask
-// tables (the rest of the CTA's shared memory stages result words).
+// Launch shape of the batched kernels: the variant, warps per CTA (variant
+// 3: 8 or 16), queries per pass (<= 512 for variant 4, <= 256 for 3) and the
+// shared-memory bytes a pass may spend on its mask tables (the rest of the
+// CTA's shared memory stages result words and row positions).
 struct BatchConfig {
-  int variant = 4;                // 4: 512-query passes, CTA-wide 1024-row blocks; 3: 256-query passes per warp
+  int variant = 4;                // 4: passes of up to 512 queries over CTA-wide blocks; 3: 256-query passes per warp
   int warps_per_cta = 16;         // variant 3 only
   int max_queries_per_pass = 512;
   size_t table_budget = 136 * 1024;

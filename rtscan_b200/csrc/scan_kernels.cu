@@ -156,15 +156,17 @@ __global__ void __launch_bounds__(kThreads) scan_fused_kernel(const __grid_const
 
 template <int NT, bool VEC>
 int max_blocks(int sm_count) {
-  static int per_sm = -1;
-  if (per_sm < 0) {
-    int b = 0;
+  static std::atomic<int> per_sm{-1};  // resident CTAs per SM (no dynamic shared memory)
+  int b = per_sm.load(std::memory_order_relaxed);
+  if (b < 0) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, scan_fused_kernel<NT, VEC>, kThreads, 0) != cudaSuccess ||
-        b < 1)
+        b < 1) {
+      cudaGetLastError();
       b = 1;
-    per_sm = b;
+    }
+    per_sm.store(b, std::memory_order_relaxed);
   }
-  return per_sm * sm_count;
+  return b * sm_count;
 }
 
 template <int NT, bool VEC>
