@@ -325,18 +325,6 @@ void *agg_scratch(rts_ctx *ctx, size_t bytes) {
   return ctx->agg_dev;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) RTS_CUDA(cudaSetDevice(dev));
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 rts_status fail(rts_ctx *ctx, const Error &e) {
   if (ctx) ctx->err = e.what();

@@ -40,16 +40,7 @@ rts_status guarded(rts_ctx *ctx, F &&f) {
   }
 }
 
-struct DeviceGuard {
-  int prev = -1, want;
-  explicit DeviceGuard(int d) : want(d) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != d) RTS_CUDA(cudaSetDevice(d));
-  }
-  ~DeviceGuard() {
-    if (prev >= 0 && prev != want) cudaSetDevice(prev);
-  }
-};
+using rts::DeviceGuard;
 
 void check_launch(rts_ctx *ctx, int n) {
   cudaError_t e = cudaGetLastError();

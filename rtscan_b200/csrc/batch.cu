@@ -970,9 +970,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       throw rts::Error(RTS_ERR_ARG, "bad batch arguments");
     const uint64_t words = rts::words_for(nrows);
     if (stride_words < words) throw rts::Error(RTS_ERR_ARG, "stride_words smaller than a bitmap");
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     if (!ctx->host_batch) ctx->host_batch = new rts::HostBatchBuffers();
     rts::HostBatchBuffers &H = *ctx->host_batch;
     if (!H.up) RTS_CUDA(cudaStreamCreateWithFlags(&H.up, cudaStreamNonBlocking));
@@ -1056,7 +1054,6 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     RTS_CUDA(cudaStreamSynchronize(H.copy));
     RTS_CUDA(cudaStreamSynchronize(H.compute));
     RTS_CUDA(cudaStreamSynchronize(H.up));
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     ctx->err = e.what();
@@ -1078,13 +1075,10 @@ extern "C" rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, 
       throw rts::Error(RTS_ERR_ARG, "bad batch arguments");
     if (stride_words < rts::words_for(ctx->nrows)) throw rts::Error(RTS_ERR_ARG, "stride_words smaller than a bitmap");
     if (nq == 0) return RTS_OK;
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     rts::batch_scan(ctx, terms, offsets, nq, dev_bitmaps, stride_words,
                     reinterpret_cast<unsigned long long *>(dev_counts), (cudaStream_t)stream,
                     ctx->batch_cfg.table_budget);
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     ctx->err = e.what();

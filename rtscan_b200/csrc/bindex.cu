@@ -644,15 +644,12 @@ rts_status rts_build_bindex(rts_ctx *ctx, int32_t column, int32_t K) {
   try {
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");
     if (column < 0 || column >= (int)ctx->cols.size()) throw rts::Error(RTS_ERR_ARG, "column out of range");
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     if (ctx->bindex.size() < ctx->cols.size()) ctx->bindex.resize(ctx->cols.size());
     ctx->bindex[column].reset();
     auto b = rts::build_bindex(ctx->cols[column], ctx->nrows, K, ctx->sm_count, nullptr);
     ctx->launches += 5;
     ctx->bindex[column] = std::move(b);
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     ctx->err = e.what();
@@ -690,14 +687,14 @@ rts_status rts_bindex_filter_vector(rts_ctx *ctx, int32_t column, int32_t k, uin
     return rts::set_thread_error(RTS_ERR_STATE, "column has no BinDex");
   const rts::GpuBinDex &B = *ctx->bindex[column];
   if (k < 0 || k >= B.K - 1 || !host_out) return rts::set_thread_error(RTS_ERR_ARG, "bad filter vector index");
-  int prev = -1;
-  cudaGetDevice(&prev);
-  if (prev != ctx->device) cudaSetDevice(ctx->device);
-  cudaError_t e = cudaMemcpy(host_out, B.fv + (uint64_t)k * B.fv_stride, rts::words_for(B.n) * 4,
-                             cudaMemcpyDeviceToHost);
-  if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
-  if (e != cudaSuccess) return rts::set_thread_error(RTS_ERR_CUDA, cudaGetErrorString(e));
-  return RTS_OK;
+  try {
+    rts::DeviceGuard device_guard(ctx->device);
+    RTS_CUDA(cudaMemcpy(host_out, B.fv + (uint64_t)k * B.fv_stride, rts::words_for(B.n) * 4,
+                        cudaMemcpyDeviceToHost));
+    return RTS_OK;
+  } catch (const rts::Error &e) {
+    return rts::set_thread_error(e.code, e.what());
+  }
 }
 
 rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
@@ -708,12 +705,9 @@ rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nt
     if (ctx->cols.empty()) throw rts::Error(RTS_ERR_STATE, "no columns loaded");
     if (!dev_bitmap || !dev_count) throw rts::Error(RTS_ERR_ARG, "null result pointer");
     if (nterms < 0 || (nterms > 0 && !terms)) throw rts::Error(RTS_ERR_ARG, "bad term list");
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     rts::bindex_query(ctx, terms, nterms, dev_bitmap, reinterpret_cast<unsigned long long *>(dev_count),
                       (cudaStream_t)stream);
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     ctx->err = e.what();

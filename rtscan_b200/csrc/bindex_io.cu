@@ -169,9 +169,7 @@ rts_status rts_save_bindex(rts_ctx *ctx, int32_t column, const char *path) {
     if (column < 0 || column >= (int)ctx->bindex.size() || !ctx->bindex[column])
       throw rts::Error(RTS_ERR_STATE, "column has no BinDex");
     const rts::GpuBinDex &B = *ctx->bindex[column];
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     unsigned long long *scratch = rts::small_device_buffer(ctx);
     rts::FileHeader h;
     memset(&h, 0, sizeof h);
@@ -206,7 +204,6 @@ rts_status rts_save_bindex(rts_ctx *ctx, int32_t column, const char *path) {
     rts::write_device(f.f, B.spos, B.n, stage.p, p);
     rts::write_device(f.f, B.fv, (uint64_t)(B.K - 1) * B.fv_stride, stage.p, p);
     if (fflush(f.f) != 0) throw rts::Error(RTS_ERR_IO, p + ": write failed");
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     return rts::fail(ctx, e.code, e.what());
@@ -248,9 +245,7 @@ rts_status rts_load_bindex(rts_ctx *ctx, int32_t column, const char *path) {
     if (h.fv_stride != (((h.n + 31) >> 5) + 3) / 4 * 4) throw rts::Error(RTS_ERR_PARSE, p + ": bad fv_stride");
     if (h.nsample != (h.n + rts::kSampleStride - 1) / rts::kSampleStride)
       throw rts::Error(RTS_ERR_PARSE, p + ": bad sample count");
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     auto b = std::make_unique<rts::GpuBinDex>();
     b->K = (int)h.K;
     b->n = h.n;
@@ -297,7 +292,6 @@ rts_status rts_load_bindex(rts_ctx *ctx, int32_t column, const char *path) {
     if (ctx->bindex.size() < ctx->cols.size()) ctx->bindex.resize(ctx->cols.size());
     ctx->bindex[column] = std::move(b);
     ctx->launches += 5;
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     return rts::fail(ctx, e.code, e.what());

@@ -114,9 +114,7 @@ rts_status rts_encode_table(rts_ctx *ctx, uint32_t encode_min, uint32_t encode_m
     if (encode_max <= encode_min || (uint64_t)(encode_max - encode_min) < n)
       throw rts::Error(RTS_ERR_ARG, "the code range must hold at least one code per row");
     const uint32_t step = (uint32_t)std::max<uint64_t>(1, ((uint64_t)encode_max - encode_min) / n);
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     const int nc = (int)ctx->cols.size();
     const uint64_t stride = (n + rts::kTileRows - 1) / rts::kTileRows * rts::kTileRows;
     auto map = std::make_unique<rts::EncodeMap>();
@@ -154,7 +152,6 @@ rts_status rts_encode_table(rts_ctx *ctx, uint32_t encode_min, uint32_t encode_m
     for (int c = 0; c < nc; c++) ctx->cols[c] = ctx->owned + (size_t)stride * c;
     ctx->encode = std::move(map);
     ctx->launches += 3 * nc;
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     return rts::fail(ctx, e.code, e.what());
@@ -185,9 +182,7 @@ rts_status rts_encode_terms(rts_ctx *ctx, const rts_term *terms, int32_t nterms,
       key[2 * i + 1] = t.hi + 1;  // U = #{values <= hi} = #{values < hi + 1}
       has[2 * i + 1] = t.hi != 0xFFFFFFFFu;
     }
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     const size_t bytes = (size_t)nc * 8 + (size_t)m * (4 + 4 + 1 + 8) + 64;
     rts::DevPtr buf;
     buf.p = rts::dev_alloc<char>(bytes);
@@ -217,7 +212,6 @@ rts_status rts_encode_terms(rts_ctx *ctx, const rts_term *terms, int32_t nterms,
         out[i].hi = E.min + (uint32_t)(U - 1) * E.step;
       }
     }
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     return RTS_OK;
   } catch (const rts::Error &e) {
     return rts::fail(ctx, e.code, e.what());

@@ -58,6 +58,21 @@ void raise_smem_limit(K kernel, std::atomic<uint64_t> &done, int bytes) {
   done.fetch_or(bit, std::memory_order_acq_rel);
 }
 
+// Make device `d` current for a scope and restore the caller's device when
+// the scope ends, on error paths too.
+struct DeviceGuard {
+  int prev = -1, want;
+  explicit DeviceGuard(int d) : want(d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != d) RTS_CUDA(cudaSetDevice(d));
+  }
+  ~DeviceGuard() {
+    if (prev >= 0 && prev != want) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 // Record `msg` as the calling thread's last error (rts_last_error(NULL)).
 rts_status set_thread_error(rts_status code, const std::string &msg);
 

@@ -137,9 +137,7 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   rts_status rc = RTS_OK;
   try {
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != ctx->device) RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     // tune on a row sample (all of a small table)
     const uint64_t sample = std::min<uint64_t>(saved_n, 1ull << 24);
     ctx->nrows = sample;
@@ -172,7 +170,6 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
     ctx->batch_cfg = best;
     ctx->nrows = saved_n;
     cache_store(cache_path, key, best, best_ms);
-    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
   } catch (const rts::Error &e) {
     ctx->nrows = saved_n;
     ctx->batch_cfg = saved_cfg;
