@@ -214,8 +214,8 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
         ctx.set_batch_config(4, 16, 513, 88 * 1024)
 
 
-@pytest.mark.parametrize("n", [70_001, 9_000_011])
-def test_batch_host_buffers(ctx, n):
+@pytest.mark.parametrize("n,nq", [(70_001, 300), (9_000_011, 300), (9_000_011, 20)])
+def test_batch_host_buffers(ctx, n, nq):
     """Host columns in, host bitmaps out: the upload, scan and download run as
     a row-chunked pipeline (two chunks at 9e6 rows), with queries outside the
     batch kernels (no term, an empty term, nine columns) among them.  The
@@ -224,7 +224,7 @@ def test_batch_host_buffers(ctx, n):
     cols = [D.uniform(n, 500 + c, [1 << 32, 1 << 20, 4096, 256, 64, 1 << 16, 1 << 32, 1000, 77][c])
             for c in range(9)]
     cols[2] = D.zipf(n, 502, 1.3)
-    qs = D.batch_queries(cols[:4], 300, seed=17) + [
+    qs = D.batch_queries(cols[:4], nq, seed=17) + [
         [], [(3, 9, 2)], [(c, 1, [1 << 31, 1 << 19, 4000, 200, 60, 1 << 15, 1 << 31, 900, 70][c]) for c in range(9)]]
     stride = R.bitmap_words(n) + 3
     bms, counts = ctx.scan_batch_host(cols, qs, stride_words=stride)
@@ -235,11 +235,14 @@ def test_batch_host_buffers(ctx, n):
     assert ctx.nrows == 1000
 
 
-def test_prepared_batch_graph_replays_match(ctx):
+@pytest.mark.parametrize("nq", [7, 100, 400])
+def test_prepared_batch_graph_replays_match(ctx, nq):
+    """Graph replays of each pass shape: term by term (7 queries), 128 slots
+    (100) and 512 slots (400), with queries outside the kernels."""
     n = 333_333
     cols = [D.uniform(n, 300), D.zipf(n, 301, 1.5), D.uniform(n, 302, 64)]
     ctx.load_columns(cols)
-    qs = D.batch_queries(cols, 400, seed=21) + [[], [(2, 9, 3)], [(c, 1, 0xFFFFFF00) for c in range(3)]]
+    qs = D.batch_queries(cols, nq, seed=21) + [[], [(2, 9, 3)], [(c, 1, 0xFFFFFF00) for c in range(3)]]
     words = R.bitmap_words(n)
     stride = (words + 31) // 32 * 32
     out = torch.full((len(qs) * stride,), -1, dtype=torch.int32, device="cuda")
