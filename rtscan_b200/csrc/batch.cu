@@ -72,6 +72,7 @@ struct BatchPass {
   uint64_t block_begin;         // first block of the range (256 rows, 1024 for variant 4)
   uint64_t nblocks;             // end of the range, in blocks
   int vec_store;                // bitmaps 16-byte aligned (out and stride)
+  uint32_t word_bytes;          // 4, passed at run time (see the mask loop of batch4_kernel)
 };
 
 // Log-linear bucket of v >= 0 with M mantissa bits: v itself below 2^M,
@@ -818,6 +819,7 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.block_begin = row_begin / rows_per_block;
     bp.nblocks = (row_end + rows_per_block - 1) / rows_per_block;
     bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
+    bp.word_bytes = 4;
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
     if (b.variant == 4) {
       if (b.cmax == 4) {

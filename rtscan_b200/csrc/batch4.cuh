@@ -280,7 +280,16 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
         uint32_t a = 0xFFFFFFFFu;
 #pragma unroll
         for (int c = 0; c < CMAX; c++)
-          if (c < C) a &= tabg[off[c]];
+          if (c < C) {
+            // 512 slots: the byte address as off * word_bytes + tabg with the
+            // multiplier a run-time 4, which compiles to a multiply-add on the
+            // FMA pipe instead of a shift-add on the busier integer ALU pipe
+            // (2 % faster per pass on B200; the smaller shapes gain nothing)
+            if (GV == 16)
+              a &= *reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(tabg) + off[c] * p.word_bytes);
+            else
+              a &= tabg[off[c]];
+          }
         acc[31 - r] = a;  // reversed: after the transpose row 0 is the MSB
       }
       transpose32(acc);
