@@ -1,7 +1,9 @@
 """GPU paths against the golden fixtures recorded from the reference itself
 (tests/golden/golden.json): the scan_cmd text goes through the product
 parser, every device path must reproduce the reference scalar filter's hit
-count and bitmap hash for every query."""
+count and bitmap hash for every query: the fused, separate and BinDex scans,
+the batched passes of every shape, the fused aggregate's count, and scans of
+the rank-encoded table with rewritten terms."""
 import hashlib
 import json
 import os
@@ -55,20 +57,34 @@ def test_golden_case(ctx, case):
             got = bm.cpu().numpy().view(np.uint32)
             assert int(cnt.item()) == q["raw_hits"], (name, q["lines"])
             assert sha(got) == q["raw_sha"], (name, q["lines"])
-    # the whole case as one batch
+    # the whole case as one batch, and repeated past 32 and 256 queries so
+    # that the table-driven pass shapes answer it too
     stride = (words + 31) // 32 * 32
-    out = torch.empty(len(queries) * stride, dtype=torch.int32, device="cuda")
-    cnts = torch.empty(len(queries), dtype=torch.int64, device="cuda")
-    for runner in (ctx.scan_each_async, ctx.scan_batch_async):
-        out.fill_(-1)
-        try:
-            runner(queries, out.data_ptr(), stride, cnts.data_ptr(), s)
-        except R.RtsError as e:
-            if e.code == -6:  # batched kernel not in this build
-                continue
-            raise
+    for reps in (1, 3, 20):
+        batch = queries * reps
+        out = torch.empty(len(batch) * stride, dtype=torch.int32, device="cuda")
+        cnts = torch.empty(len(batch), dtype=torch.int64, device="cuda")
+        for runner in ((ctx.scan_each_async, ctx.scan_batch_async) if reps == 1 else (ctx.scan_batch_async,)):
+            out.fill_(-1)
+            runner(batch, out.data_ptr(), stride, cnts.data_ptr(), s)
+            torch.cuda.synchronize()
+            o = out.cpu().numpy().view(np.uint32)
+            for i in range(len(batch)):
+                q = case["queries"][i % len(queries)]
+                assert int(cnts[i].item()) == q["raw_hits"], (runner.__name__, reps, q["lines"])
+                assert sha(o[i * stride:i * stride + words]) == q["raw_sha"], (runner.__name__, reps, q["lines"])
+    # the fused scan-and-aggregate's count
+    s2 = torch.zeros(2, dtype=torch.int64, device="cuda")
+    for terms, q in zip(queries, case["queries"]):
+        if len({t[0] for t in terms}) <= 8:
+            ctx.scan_aggregate_async(terms, -1, -1, cnt.data_ptr(), s2.data_ptr(), s)
+            torch.cuda.synchronize()
+            assert int(cnt.item()) == q["raw_hits"], ("aggregate", q["lines"])
+    # the rank-encoded table with rewritten terms
+    ctx.encode_table()
+    for terms, q in zip(queries, case["queries"]):
+        bm.fill_(-1)
+        ctx.scan_async(ctx.encode_terms(terms), bm.data_ptr(), cnt.data_ptr(), s)
         torch.cuda.synchronize()
-        o = out.cpu().numpy().view(np.uint32)
-        for i, q in enumerate(case["queries"]):
-            assert int(cnts[i].item()) == q["raw_hits"], (runner.__name__, q["lines"])
-            assert sha(o[i * stride:i * stride + words]) == q["raw_sha"], (runner.__name__, q["lines"])
+        assert int(cnt.item()) == q["raw_hits"], ("encoded", q["lines"])
+        assert sha(bm.cpu().numpy().view(np.uint32)) == q["raw_sha"], ("encoded", q["lines"])
