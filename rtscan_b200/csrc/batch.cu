@@ -362,6 +362,14 @@ size_t smem_bytes4(uint32_t blob_words) {
   return ((blob_words + 3) & ~3u) * 4 + (size_t)kV4StageWords * 4 + (size_t)kV4PosBytes<CMAX, GV>;
 }
 
+// Shared memory of a variant-4 pass: `groups` slot groups over up to `cmax`
+// columns, blob of `blob_words` words.
+size_t pass_smem4(size_t blob_words, int cmax, int groups) {
+  const uint32_t w = (uint32_t)std::min<size_t>(blob_words, 1u << 30);
+  if (cmax <= 4) return groups == 4 ? smem_bytes4<4, 4>(w) : groups == 8 ? smem_bytes4<4, 8>(w) : smem_bytes4<4, 16>(w);
+  return groups == 4 ? smem_bytes4<8, 4>(w) : groups == 8 ? smem_bytes4<8, 8>(w) : smem_bytes4<8, 16>(w);
+}
+
 template <int CMAX, int GV>
 void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
   static std::atomic<uint64_t> raised{0};
@@ -733,7 +741,21 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       for (uint32_t pos = 0; pos <= m; pos++)
         for (int grp = 0; grp < Gp; grp++) tab[(size_t)pos * Gp + grp] = acc[grp] ^= delta[c][(size_t)pos * Gp + grp];
     }
-    // boundaries and bucket index
+    // boundaries and bucket index.  The table budget counts 4 buckets per
+    // boundary; a pass takes 16 where its shared memory still holds them:
+    // fewer boundaries per bucket make more loop-free lookups exact and the
+    // searches shorter.
+    auto buckets_for = [](uint32_t m, uint32_t per) {
+      uint32_t nb = 1;
+      while (nb < per * m && nb < 4096) nb <<= 1;
+      return nb;
+    };
+    uint32_t per = 4;
+    if (variant == 4) {
+      size_t w = blob.size() + 32 * (size_t)Gp;  // tables so far, slot map
+      for (int c = 0; c < C; c++) w += bp.m[c] + (bp.m[c] ? (buckets_for(bp.m[c], 16) + 3) / 2 : 1);
+      if (pass_smem4(w, C <= 4 ? 4 : 8, Gp) <= 227 * 1024) per = 16;
+    }
     for (int c = 0; c < C; c++) {
       const uint32_t m = bp.m[c];
       bp.bnd_off[c] = (uint32_t)blob.size();
@@ -747,9 +769,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       bp.bmin[c] = B[c].front();
       bp.bmax[c] = B[c].back();
       const uint64_t span = (uint64_t)bp.bmax[c] - bp.bmin[c] + 1;
-      uint32_t nb_target = 1;
-      while (nb_target < 4 * m && nb_target < 4096) nb_target <<= 1;
-      const std::vector<uint16_t> bk = bucket_index(B[c], span, nb_target, &bp.shift[c], &bp.lgm[c]);
+      const std::vector<uint16_t> bk = bucket_index(B[c], span, buckets_for(m, per), &bp.shift[c], &bp.lgm[c]);
       bp.nbk[c] = (uint32_t)bk.size() - 1;
       bp.bkt_off[c] = (uint32_t)blob.size();
       const size_t wsz = (bk.size() + 1) / 2;

@@ -138,26 +138,13 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
       for (int c = 0; c < CMAX; c++) val[h][c] = (c < C && row < p.nrows) ? __ldg(p.col[c] + row) : 0u;
     }
   };
+  // kAhead: latency hidden behind the masks, so the search with the fewest
+  // instructions
   auto row_offsets = [&](uint64_t b, int h, uint32_t(&off)[CMAX]) {
     const bool in = b * S::kRows + threadIdx.x + h * kV4Threads < p.nrows;
     uint32_t pos[CMAX];
-    if (kAhead) {  // latency hidden behind the masks: the search with the fewest instructions
 #pragma unroll
-      for (int c = 0; c < CMAX; c++) pos[c] = (c < C && in) ? position(p, blob, c, val[h][c]) : 0u;
-    } else {  // loop-free lookups that overlap one another, full search when a bucket is crowded
-      bool exact = true;
-#pragma unroll
-      for (int c = 0; c < CMAX; c++) {
-        bool e = true;
-        pos[c] = (c < C && in) ? position_fast(p, blob, c, val[h][c], e) : 0u;
-        exact = exact && e;
-      }
-      if (!exact) {
-#pragma unroll
-        for (int c = 0; c < CMAX; c++)
-          if (c < C) pos[c] = position(p, blob, c, val[h][c]);
-      }
-    }
+    for (int c = 0; c < CMAX; c++) pos[c] = (c < C && in) ? position(p, blob, c, val[h][c]) : 0u;
 #pragma unroll
     for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[c] * GV : 0u;
   };
@@ -171,6 +158,49 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
       for (int c = 0; c < CMAX; c += 4)
         *reinterpret_cast<uint2 *>(dst + c) =
             make_uint2(off[c] | (off[(c + 1) % CMAX] << 16), off[(c + 2) % CMAX] | (off[(c + 3) % CMAX] << 16));
+    }
+  };
+  // Other shapes: loop-free lookups for up to 32 (row, column) pairs at once,
+  // so that their shared-memory loads overlap, and their offsets to shared
+  // memory; then the full search for the few whose bucket is crowded, each
+  // lane over its own misses only (a column value read again, from cache),
+  // overwriting those entries.
+  auto block_offsets = [&](uint64_t b) {
+    constexpr int H = (32 / CMAX) < S::kRPT ? (32 / CMAX) : S::kRPT;  // rows per batch of lookups
+#pragma unroll
+    for (int h0 = 0; h0 < S::kRPT; h0 += H) {
+      uint32_t pos[H][CMAX];
+      uint32_t miss[CMAX];  // bit hh: the lookup of (row h0 + hh, column c) was not exact
+#pragma unroll
+      for (int c = 0; c < CMAX; c++) miss[c] = 0;
+#pragma unroll
+      for (int hh = 0; hh < H; hh++) {
+        const bool in = b * S::kRows + threadIdx.x + (h0 + hh) * kV4Threads < p.nrows;
+#pragma unroll
+        for (int c = 0; c < CMAX; c++) {
+          bool e = true;
+          pos[hh][c] = (c < C && in) ? position_fast(p, blob, c, val[h0 + hh][c], e) : 0u;
+          miss[c] |= (e ? 0u : 1u) << hh;
+        }
+      }
+#pragma unroll
+      for (int hh = 0; hh < H; hh++) {
+        uint32_t off[CMAX];
+#pragma unroll
+        for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[hh][c] * GV : 0u;
+        put_row(h0 + hh, off);
+      }
+#pragma unroll
+      for (int c = 0; c < CMAX; c++) {
+        uint32_t mc = miss[c];
+        while (mc) {
+          const int hh = __ffs(mc) - 1;
+          mc &= mc - 1;
+          const int r = threadIdx.x + (h0 + hh) * kV4Threads;
+          const uint32_t x = __ldg(p.col[c] + b * S::kRows + r);
+          posbuf[(r + (r >> 5)) * CMAX + c] = (V4Pos<CMAX>)(p.tab_off[c] + position(p, blob, c, x) * GV);
+        }
+      }
     }
   };
   auto find_offsets = [&](uint64_t b) {  // kAhead: into offn
@@ -210,12 +240,7 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
         put_offsets();
       } else {
         load_values(blk);
-#pragma unroll
-        for (int h = 0; h < S::kRPT; h++) {
-          uint32_t off[CMAX];
-          row_offsets(blk, h, off);
-          put_row(h, off);
-        }
+        block_offsets(blk);
       }
     }
     if (prev != ~0ull) {

@@ -115,10 +115,12 @@ def test_batch_pass_shapes_at_block_edges(ctx, nq):
         check_batch(ctx, cols, D.batch_queries(cols, nq, seed=n + nq))
 
 
-def test_batch_skewed_boundaries(ctx):
+@pytest.mark.parametrize("nq", [100, 200, 500])
+def test_batch_skewed_boundaries(ctx, nq):
     """Bounds packed into small values plus powers of two up to 2^32 - 1 (the
     shape for which the planner indexes boundaries by log-linear buckets),
-    with rows sitting on and next to every bound."""
+    with rows sitting on and next to every bound; crowded buckets send many
+    rows to the full search in every pass shape (128, 256 and 512 slots)."""
     n = 120_000
     rng = np.random.default_rng(5)
     edges = [0, 1, 2] + [v for k in range(2, 33) for v in ((1 << k) - 2, (1 << k) - 1, 1 << k)
@@ -133,7 +135,7 @@ def test_batch_skewed_boundaries(ctx):
     ctx.load_columns(cols)
     pool = [int(e) for e in edges] + list(range(0, 400, 3))
     qs = []
-    for i in range(500):
+    for i in range(nq):
         a, b = sorted(int(x) for x in rng.choice(pool, size=2))
         q = [(0, a, b)]
         if i % 3 == 0:
