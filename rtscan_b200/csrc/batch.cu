@@ -20,7 +20,7 @@
 //   * Variant 4 (default, batch4.cuh): CTA-wide blocks of 1024-4096 rows;
 //     each lane ANDs the masks of 32 rows for one group, transposes the
 //     32x32 bit block in registers and stages the words for whole-line
-//     stores.  Passes of at most 32 queries skip the tables and test each
+//     stores.  Passes of at most 20 queries skip the tables and test each
 //     term directly (batch_few.cuh).  Variant 3 (below): 256-query passes
 //     with one 256-row block per warp, kept as an autotuner candidate.
 //   * Counts are kept per lane in registers and flushed once per CTA.
@@ -539,7 +539,7 @@ struct BatchPlan {
     int cmax;
     int variant;  // kernel the pass was planned for (3: 256-slot warps, 4: CTA-wide blocks)
     int groups;   // 32-slot groups of the pass (table words per position)
-    bool few;     // at most 32 queries: tested term by term (batch_few_kernel), no tables
+    bool few;     // at most kFewMaxQueries queries: tested term by term (batch_few_kernel), no tables
     FewPass fp;
   };
   std::vector<Pass> passes;
@@ -665,7 +665,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     memset(&b.fp, 0, sizeof b.fp);
     b.few = false;
     const int C = (int)pp.cols.size();
-    if (variant == 4 && (int)pp.qs.size() <= kFewSlots) {
+    if (variant == 4 && (int)pp.qs.size() <= kFewMaxQueries) {
       FewPass &fp = b.fp;
       b.few = true;
       b.variant = variant;
@@ -674,13 +674,15 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       fp.nq = (int)pp.qs.size();
       fp.ncols = C;
       for (int c = 0; c < C; c++) fp.col[c] = ctx->cols[pp.cols[c]];
-      for (int j = 0; j < kFewSlots; j++) fp.slot_query[j] = -1;
+      for (int j = 0; j < kFewSlots; j++) {
+        fp.slot_query[j] = -1;
+        for (int c = 0; c < kMaxCols; c++) fp.term[j][c] = make_uint2(0u, 0xFFFFFFFFu);  // always true
+      }
       for (int j = 0; j < fp.nq; j++) {
         const NormQuery &q = norm[pp.qs[j]];
         fp.slot_query[j] = out_index ? out_index[pp.qs[j]] : pp.qs[j];
         for (size_t k = 0; k < q.cols.size(); k++) {
           const int c = (int)(std::find(pp.cols.begin(), pp.cols.end(), q.cols[k]) - pp.cols.begin());
-          fp.colmask[j] |= 1u << c;
           fp.term[j][c] = make_uint2(q.lo[k], q.hi[k] - q.lo[k]);
         }
       }
@@ -813,14 +815,14 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
       const uint64_t ctas = (fp.ntiles - fp.tile_begin + kFewWarps - 1) / kFewWarps;
       const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)ctx->sm_count * 8));
       switch (fp.ncols) {
-        case 1: batch_few_kernel<1><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 2: batch_few_kernel<2><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 3: batch_few_kernel<3><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 4: batch_few_kernel<4><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 5: batch_few_kernel<5><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 6: batch_few_kernel<6><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        case 7: batch_few_kernel<7><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
-        default: batch_few_kernel<8><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+        case 1: launch_few<1>(fp, grid, s); break;
+        case 2: launch_few<2>(fp, grid, s); break;
+        case 3: launch_few<3>(fp, grid, s); break;
+        case 4: launch_few<4>(fp, grid, s); break;
+        case 5: launch_few<5>(fp, grid, s); break;
+        case 6: launch_few<6>(fp, grid, s); break;
+        case 7: launch_few<7>(fp, grid, s); break;
+        default: launch_few<8>(fp, grid, s); break;
       }
       launches++;
       continue;

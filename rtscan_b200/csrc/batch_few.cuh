@@ -4,19 +4,25 @@
 // With few queries the table-driven kernel's per-row work (interval
 // positions, table loads, bit transposes) is shared by too few queries to
 // pay off, so each row is tested against each term directly: a lane holds
-// one row's column values, the terms of a chunk of queries sit in
-// registers, and one ballot per query and 32 rows gives a result word.  A
-// warp covers a 1024-row tile: the 32 ballots of a query are collected in
-// shared memory and leave as one 128-byte line per query.  Cost per row and
-// query is two instructions per pass column plus about three, against the
-// columns' read traffic.
+// one row's column values, and one ballot per query and 32 rows gives a
+// result word.  A warp covers a 1024-row tile in chunks of Q queries whose
+// terms it reads from the kernel parameters; lane t keeps the ballot of
+// rows 32t .. 32t+31 of each query of the chunk, so a query's 32 words
+// leave as one 128-byte line straight from registers.  Q is a template
+// parameter chosen per pass (few_chunk()): the pass's own count for one or
+// two queries, else the most that the column count leaves room for.  One
+// chunk size per kernel: a kernel holding several ran its main chunk
+// 5-9 % slower on B200.
 constexpr int kFewSlots = 32;
+// Passes of at most this many queries run term by term.  On one 2^23-row
+// segment of 4 columns the term-by-term kernel takes about 134 us at 16
+// queries and 185 us at 24, a 128-slot table pass 160-165 us at any count.
+constexpr int kFewMaxQueries = 20;
 constexpr int kFewWarps = 8;
 
 struct FewPass {
   const uint32_t *col[kMaxCols];
-  uint2 term[kFewSlots][kMaxCols];  // (lo, hi - lo) of slot s on pass column c
-  uint32_t colmask[kFewSlots];      // pass columns slot s constrains
+  uint2 term[kFewSlots][kMaxCols];  // (lo, hi - lo) of slot s on pass column c; (0, 2^32 - 1) if unconstrained
   int32_t slot_query[kFewSlots];    // bitmap index of slot s, -1 when unused
   int nq;
   int ncols;
@@ -29,36 +35,38 @@ struct FewPass {
   uint64_t ntiles;      // end of the range, in tiles
 };
 
+// Queries per chunk for a pass of nq queries over C columns.  Each chunk
+// reads the tile's columns once (from L1/L2 after the first), so fewer
+// columns leave room for more queries per chunk.
 template <int C>
+constexpr int few_chunk_max() { return C <= 2 ? 8 : C <= 4 ? 4 : 2; }
+inline int few_chunk(int nq, int ncols) {
+  const int q = ncols <= 2 ? 8 : ncols <= 4 ? 4 : 2;
+  return nq < q ? (nq <= 1 ? 1 : nq <= 2 ? 2 : q) : q;
+}
+
+template <int C, int Q>
 __global__ void __launch_bounds__(kFewWarps * 32, 4) batch_few_kernel(const __grid_constant__ FewPass p) {
-  // Queries go in chunks of QCH whose terms sit in registers (lo, hi - lo per
-  // column; an unconstrained column has (0, 2^32 - 1), always true); the
-  // chunk's 1024-row tile is read once per chunk (from L1/L2 after the first).
-  constexpr int QCH = C <= 2 ? 8 : C <= 4 ? 4 : 2;
-  __shared__ uint32_t stage[kFewWarps][kFewSlots][32];
-  __shared__ uint2 term[kFewSlots][C];
   __shared__ unsigned long long cnt[kFewSlots];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x < kFewSlots) {
-    cnt[threadIdx.x] = 0;
-    const bool used = threadIdx.x < p.nq;
-#pragma unroll
-    for (int c = 0; c < C; c++)
-      term[threadIdx.x][c] = !used ? make_uint2(1u, 0u)  // never true: the slot is unused
-                             : (p.colmask[threadIdx.x] >> c & 1) ? p.term[threadIdx.x][c]
-                                                                  : make_uint2(0u, 0xFFFFFFFFu);
-  }
+  if (threadIdx.x < kFewSlots) cnt[threadIdx.x] = 0;
   __syncthreads();
   const int nq = p.nq;
   const uint64_t gw = (uint64_t)blockIdx.x * kFewWarps + warp, nw = (uint64_t)gridDim.x * kFewWarps;
+  unsigned long long mine = 0;  // lane j: matches of query j in this warp's tiles
   for (uint64_t tile = p.tile_begin + gw; tile < p.ntiles; tile += nw) {
-    const uint64_t row0 = tile * 1024;
-    for (int j0 = 0; j0 < nq; j0 += QCH) {
-      uint2 tm[QCH][C];
+    const uint64_t row0 = tile * 1024, word = tile * 32 + lane;
+    for (int j0 = 0; j0 < nq; j0 += Q) {
+      // slots past nq (the last chunk's) hold always-true terms; their
+      // results are neither stored nor counted
+      uint2 tm[Q][C];
 #pragma unroll
-      for (int jj = 0; jj < QCH; jj++)
+      for (int jj = 0; jj < Q; jj++)
 #pragma unroll
-        for (int c = 0; c < C; c++) tm[jj][c] = term[(j0 + jj) & (kFewSlots - 1)][c];
+        for (int c = 0; c < C; c++) tm[jj][c] = p.term[(j0 + jj) & (kFewSlots - 1)][c];
+      uint32_t r[Q];  // lane t: the ballot of rows row0 + 32t .. row0 + 32t + 31
+#pragma unroll
+      for (int jj = 0; jj < Q; jj++) r[jj] = 0;
       uint32_t nxt[C];
       auto load = [&](int t) {
         const uint64_t row = row0 + t * 32 + lane;
@@ -72,28 +80,41 @@ __global__ void __launch_bounds__(kFewWarps * 32, 4) batch_few_kernel(const __gr
         for (int c = 0; c < C; c++) v[c] = nxt[c];
         if (t + 1 < 32) load(t + 1);
         const bool in = row0 + t * 32 + lane < p.nrows;
+        const bool own = lane == t;
 #pragma unroll
-        for (int jj = 0; jj < QCH; jj++) {
+        for (int jj = 0; jj < Q; jj++) {
           bool pass = in;
 #pragma unroll
           for (int c = 0; c < C; c++) pass = pass && (v[c] - tm[jj][c].x <= tm[jj][c].y);
-          const uint32_t w = __brev(__ballot_sync(kFull, pass));  // row t*32 + i -> bit 31 - i
-          if (lane == 0 && j0 + jj < nq) stage[warp][j0 + jj][t] = w;
+          const uint32_t b = __ballot_sync(kFull, pass);
+          r[jj] = own ? b : r[jj];
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < Q; jj++) {
+        const int j = j0 + jj;
+        if (j < nq) {
+          const uint32_t w = __brev(r[jj]);  // row 32t + i -> bit 31 - i
+          const int32_t sq = p.slot_query[j];
+          if (sq >= 0 && word < p.words) p.out[(uint64_t)sq * p.stride_words + word] = w;
+          const uint32_t total = __reduce_add_sync(kFull, (uint32_t)__popc(w));
+          if (lane == j) mine += total;
         }
       }
     }
-    __syncwarp();
-    const uint64_t word = tile * 32 + lane;
-    for (int j = 0; j < nq; j++) {
-      const uint32_t w = stage[warp][j][lane];
-      const int32_t sq = p.slot_query[j];
-      if (sq >= 0 && word < p.words) p.out[(uint64_t)sq * p.stride_words + word] = w;
-      const uint32_t total = __reduce_add_sync(kFull, (uint32_t)__popc(w));
-      if (lane == 0 && total) atomicAdd(&cnt[j], (unsigned long long)total);
-    }
-    __syncwarp();
   }
+  if (lane < nq && mine) atomicAdd(&cnt[lane], mine);
   __syncthreads();
   if (threadIdx.x < nq && cnt[threadIdx.x] && p.slot_query[threadIdx.x] >= 0)
     atomicAdd(p.counts + p.slot_query[threadIdx.x], cnt[threadIdx.x]);
+}
+
+template <int C>
+void launch_few(const FewPass &fp, int grid, cudaStream_t s) {
+  constexpr int Q = few_chunk_max<C>();
+  switch (few_chunk(fp.nq, C)) {
+    case 1: batch_few_kernel<C, 1><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+    case 2: batch_few_kernel<C, 2><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+    default: batch_few_kernel<C, Q><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
+  }
 }
