@@ -803,6 +803,28 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
                 unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
   int launches = 0;
   for (auto &b : plan.passes) {
+    if (b.few && b.fp.nq == 1 && b.fp.slot_query[0] >= 0) {
+      // one query: the single-query scan kernel over the range, which runs at
+      // HBM speed (the term-by-term kernel reaches about half of it here);
+      // the range starts at a multiple of 4096 rows, so the column and
+      // bitmap offsets keep their alignment, and the count accumulates
+      const FewPass &f = b.fp;
+      ScanParams sp;
+      memset(&sp, 0, sizeof sp);
+      bool vec = true;
+      for (int c = 0; c < f.ncols; c++) {
+        sp.t[c] = {f.col[c] + row_begin, f.term[0][c].x, f.term[0][c].y};
+        vec = vec && (((uintptr_t)sp.t[c].col & 15) == 0);
+      }
+      sp.nterms = f.ncols;
+      sp.out = out + (uint64_t)f.slot_query[0] * stride_words + row_begin / 32;
+      sp.count = counts + f.slot_query[0];
+      sp.nrows = row_end - row_begin;
+      sp.full_tiles = sp.nrows / kTileRows;
+      launch_scan_fused(sp, vec, ctx->sm_count, s);
+      launches++;
+      continue;
+    }
     if (b.few) {
       FewPass fp = b.fp;
       fp.out = out;
