@@ -21,8 +21,8 @@
 //      for the block (128 bytes per 1024 rows) leave as 16-byte stores from
 //      128 / GV lanes, whole 128-byte lines.
 // No cross-lane exchange is needed, and positions are shared by all queries
-// of the pass.  For 512-slot passes over up to 4 columns, step 1 for the
-// next block runs inside step 2 (see the kernel).
+// of the pass.  For 512- and 256-slot passes over up to 4 columns, step 1
+// for the next block runs inside step 2 (see the kernel).
 constexpr int kV4Warps = 16;
 constexpr int kV4Threads = kV4Warps * 32;
 constexpr int kV4StageWords = 16384;  // 64 KB: slots x words per query per block, for every GV
@@ -120,14 +120,16 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
 #pragma unroll
   for (int i = 0; i < 8; i++) cnt[i] = 0;
 
-  // For 512-slot passes over up to 4 columns, positions are found one block
-  // ahead, inside step 2: even warps before their masks, odd warps after, so
+  // For 512- and 256-slot passes over up to 4 columns (3-5 % faster for the
+  // 256-slot shape, 4-10 % slower for the 128-slot one, whose 8 rows per
+  // thread are too many to hold), positions are found one block ahead,
+  // inside step 2: even warps before their masks, odd warps after, so
   // the dependent shared-memory loads of the boundary search overlap other
   // warps' mask arithmetic; the table word offsets wait in registers as
   // 16-bit pairs until the next step 1 writes them to shared memory, and the
   // column values are loaded one more block ahead.  Other shapes find the
   // positions of a block in its own step 1.
-  constexpr bool kAhead = GV == 16 && CMAX <= 4;
+  constexpr bool kAhead = (GV == 16 || GV == 8) && CMAX <= 4;
   uint32_t val[S::kRPT][CMAX];                    // column values of this thread's rows
   uint32_t offn[kAhead ? S::kRPT : 1][(CMAX + 1) / 2];  // their table word offsets, two per register
   auto load_values = [&](uint64_t b) {
