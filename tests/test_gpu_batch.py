@@ -46,7 +46,7 @@ def check_batch(ctx, cols, queries):
         assert (pad == 0xFFFFFFFF).all(), "wrote past the bitmap"
 
 
-@pytest.mark.parametrize("nq", [1, 5, 31, 32, 33, 255, 256, 257, 700])
+@pytest.mark.parametrize("nq", [1, 2, 5, 20, 21, 31, 32, 33, 255, 256, 257, 700])
 def test_batch_sizes(ctx, nq):
     n = 300_000 + 123
     cols = [D.uniform(n, 1), D.zipf(n, 2, 1.3), D.uniform(n, 3, 256), D.normal(n, 4)]
@@ -216,11 +216,13 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
         ctx.set_batch_config(4, 16, 513, 88 * 1024)
 
 
-@pytest.mark.parametrize("n,nq", [(70_001, 300), (9_000_011, 300), (9_000_011, 20)])
+@pytest.mark.parametrize("n,nq", [(70_001, 300), (9_000_011, 300), (9_000_011, 20), (9_000_011, 2),
+                                  (9_000_011, 1)])
 def test_batch_host_buffers(ctx, n, nq):
     """Host columns in, host bitmaps out: the upload, scan and download run as
     a row-chunked pipeline (two chunks at 9e6 rows), with queries outside the
-    batch kernels (no term, an empty term, nine columns) among them.  The
+    batch kernels (no term, an empty term, nine columns) among them; one
+    kernel query runs as a fused scan per chunk, two term by term.  The
     context's own table is untouched."""
     ctx.load_columns([D.uniform(1000, 1)])
     cols = [D.uniform(n, 500 + c, [1 << 32, 1 << 20, 4096, 256, 64, 1 << 16, 1 << 32, 1000, 77][c])
