@@ -494,6 +494,8 @@ def run(args):
 
     if args.bindex_io and rank == 0:
         line["bindex_io"] = bindex_io_leg(torch, R, dev, args.bindex_io)
+    if args.bindex_query and rank == 0:
+        line["bindex_query"] = bindex_query_leg(torch, R, D, dev, args.bindex_query)
 
     if wl == "batched" and args.pass_sweep:
         line["pass_sweep"] = pass_sweep(torch, R, D, dev, rank, args.pass_sweep)
@@ -560,6 +562,90 @@ def bindex_io_leg(torch, R, dev, n, K=128):
     return {"rows": n, "K": K, "file_MB": round(size / 1e6, 1), "build_ms": round(build_s * 1e3, 1),
             "save_ms": round(save_s * 1e3, 1), "load_ms": round(load_s * 1e3, 1),
             "load_GB_s": round(size / load_s / 1e9, 2)}
+
+
+def bindex_query_leg(torch, R, D, dev, n, K=128):
+    """Single-column queries through the BinDex against fused scans of the
+    same queries, on a uniform column at 0.1/1/10/50/90 % selectivity and on
+    a column of 256 values (the single-column sweep's shapes): CUDA-event
+    medians on one stream, and each BinDex bitmap checked equal to the fused
+    scan's.  `rows_per_s` is n over the BinDex time.  `GB_s` credits the
+    bytes of the plan the BinDex planner picks, costed the way bindex_query
+    (csrc/bindex.cu) costs it, here from exact ranks: the result write,
+    every filter vector read, and 12 B per re-tested row (its row id, its
+    gathered value and its result word).  A query whose matches are cheaper
+    to re-test than to sieve starts from zero and re-tests those rows only
+    ("refine_only")."""
+    s = torch.cuda.current_stream()
+    bm = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    ref = torch.empty_like(bm)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    res = {"rows": n, "K": K, "queries": []}
+
+    def timed(fn, reps=7):
+        for _ in range(3):
+            fn()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return sorted(ts)[reps // 2]
+
+    for kind, seed in (("uniform", 31), ("range:0:256", 41)):
+        col = gpu_column(torch, kind, n, seed, dev)
+        c = R.Context(dev.index or 0)
+        c.attach_columns([col.data_ptr()], n)
+        c.build_bindex(0, K)
+        srt = torch.sort(col.to(torch.int64) & 0xFFFFFFFF).values
+        lower = lambda b: int(torch.searchsorted(srt, torch.tensor([b], device=dev)).item())
+        fr = [lower(int(srt[k * (n // K)].item())) for k in range(K)]  # rank of area k's start value
+
+        def nearest(est):  # the planner's filter vector (or constant) nearest to rank est
+            best, bd = (-1, 0), est
+            if n - est < bd:
+                best, bd = (K - 1, n), n - est
+            for j in range(1, K):
+                if abs(fr[j] - est) < bd:
+                    best, bd = (j - 1, fr[j]), abs(fr[j] - est)
+            return best
+
+        if kind == "uniform":
+            smp = host_sample(torch, col)
+            qs = [D.range_for_selectivity(smp, sel) for sel in (0.001, 0.01, 0.10, 0.50, 0.90)]
+        else:
+            qs = [(3, 3), (0, 25), (64, 191), (10, 250)]
+        for lo, hi in qs:
+            terms = [(0, lo, hi)]
+            r_lo = lower(lo) if lo > 0 else 0
+            r_hi = lower(hi + 1) if hi < 0xFFFFFFFF else n
+            refine, fv_reads = 0, 0
+            for has, r in ((lo > 0, r_lo), (hi < 0xFFFFFFFF, r_hi)):
+                if has:
+                    k, rk = nearest(r)
+                    refine += abs(rk - r)
+                    fv_reads += 0 <= k < K - 1
+            match = max(0, r_hi - r_lo)
+            sieve_cost = n / 8 * (1 + fv_reads) + refine * 40.0
+            cand_cost = n / 8 + (match + 2048) * 40.0
+            refine_only = cand_cost < sieve_cost
+            nbytes = n / 8 + match * 12 if refine_only else n / 8 * (1 + fv_reads) + refine * 12
+            t_b = timed(lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream))
+            hits = int(cnt.item())
+            t_f = timed(lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream))
+            res["queries"].append({
+                "column": kind, "lo": lo, "hi": hi, "selectivity": round(hits / n, 5),
+                "bindex_us": round(t_b * 1e3, 1), "fused_us": round(t_f * 1e3, 1),
+                "rows_per_s": round(n / (t_b * 1e-3), 1), "plan": "refine_only" if refine_only else "sieve",
+                "refined_rows": match if refine_only else refine, "bytes_MB": round(nbytes / 1e6, 2),
+                "GB_s": round(nbytes / (t_b * 1e-3) / 1e9, 1), "equal": bool(torch.equal(bm, ref))})
+        c.close()
+        del col, srt
+        torch.cuda.empty_cache()
+    return res
 
 
 def q6_legs(torch, R, ctx, terms, n, out, cnt, s, timed, fused_ms):
@@ -760,6 +846,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch launch shape")
     ap.add_argument("--bindex-io", type=int, default=0, metavar="ROWS",
                     help="also time BinDex build vs save and load for a ROWS-row column (off by default)")
+    ap.add_argument("--bindex-query", type=int, default=0, metavar="ROWS",
+                    help="also time single-column BinDex queries against fused scans on ROWS-row columns")
     ap.add_argument("--pass-sweep", type=int, default=0, metavar="ROWS",
                     help="also time one pass of 1..512 queries over a ROWS-row table (off by default)")
     ap.add_argument("--serve-rows", type=int, default=1 << 28)

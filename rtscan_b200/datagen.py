@@ -73,13 +73,12 @@ def range_for_selectivity(sample_sorted: np.ndarray, sel: float, center: float =
     """Inclusive [lo, hi] covering about `sel` of the rows, from sample
     quantiles [q(center - sel/2), q(center + sel/2)]."""
     m = len(sample_sorted)
-    a = max(0.0, center - sel / 2)
-    b = min(1.0, center + sel / 2)
-    if b - a < sel:  # pushed against an end
-        if a == 0.0:
-            b = min(1.0, sel)
-        else:
-            a = max(0.0, 1.0 - sel)
+    a = center - sel / 2
+    b = center + sel / 2
+    if a < 0.0:  # pushed against an end: keep the width
+        a, b = 0.0, min(1.0, sel)
+    elif b > 1.0:
+        a, b = max(0.0, 1.0 - sel), 1.0
     lo = int(sample_sorted[min(m - 1, int(a * m))])
     hi = int(sample_sorted[min(m - 1, max(0, int(math.ceil(b * m)) - 1))])
     return lo, max(lo, hi)
