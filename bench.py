@@ -470,12 +470,7 @@ def run(args):
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic (seeded, generated on device)",
-        "config": {"workload": {"batched": f"batched scan {n:.3g} rows x 4 skewed columns, {nq} queries",
-                                "single": f"single-column {n:.3g}-row scan, 10% selectivity",
-                                "multi": f"4-column {n:.3g}-row conjunctive scan",
-                                "q6": f"fused scan-and-aggregate, {n:.3g} rows x 4 columns (TPC-H Q6 shape)"}[wl],
-                   "nrows_per_gpu": n, "ncols": len(cols), "queries_per_step": nq,
-                   "column_kinds": kinds, "l2": f"inputs larger than L2 ({n * 4 / 1e6:.0f} MB per column)"},
+        "config": workload_config(wl, n, nq, kinds),
         "queries_per_s": round(nq * world / (ms_step * 1e-3), 1),
         "rows_per_s": round(n * world / (ms_step * 1e-3), 1),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
@@ -784,6 +779,18 @@ def served_leg(torch, R, D, ctx, dev, rank, args):
     return out
 
 
+def workload_config(wl, n, nq, kinds):
+    """The `config` object of both arms' lines: the workload a step stands
+    for (the reference arm times bounded samples of it, described in its
+    cpu_baseline.sample)."""
+    name = {"batched": f"batched scan {n:.3g} rows x 4 skewed columns, {nq} queries",
+            "single": f"single-column {n:.3g}-row scan, 10% selectivity",
+            "multi": f"4-column {n:.3g}-row conjunctive scan",
+            "q6": f"fused scan-and-aggregate, {n:.3g} rows x 4 columns (TPC-H Q6 shape)"}[wl]
+    return {"workload": name, "nrows_per_gpu": n, "ncols": len(kinds), "queries_per_step": nq,
+            "column_kinds": kinds, "l2": f"inputs larger than L2 ({n * 4 / 1e6:.0f} MB per column)"}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU path on this host, rank 0 only."""
     world, rank, _ = dist_env()
@@ -816,8 +823,7 @@ def run_reference(args):
             "steps": len(vals), "warmup": args.warmup, "ms_per_step": round(1e3 * per_step / qps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)",
-            "config": {"workload": wl, "nrows": REF_N, "ncols": len(cols), "queries_per_step": per_step,
-                       "column_kinds": kinds},
+            "config": workload_config(wl, args.nrows, len(queries), kinds),
             "queries_per_s": round(qps * REF_N / args.nrows, 3),
             "queries_per_s_sample": round(qps, 2),
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "kind": kind, "cores": cores,

@@ -1,5 +1,6 @@
-// Batched kernel for passes of at most 32 queries (included by batch.cu
-// inside its anonymous namespace; uses kFull and kMaxCols from there).
+// Batched kernel for passes of few queries: at most 32 slots, and the
+// planner sends passes of up to kFewMaxQueries (included by batch.cu inside
+// its anonymous namespace; uses kFull and kMaxCols from there).
 //
 // With few queries the table-driven kernel's per-row work (interval
 // positions, table loads, bit transposes) is shared by too few queries to
@@ -35,13 +36,13 @@ struct FewPass {
   uint64_t ntiles;      // end of the range, in tiles
 };
 
-// Queries per chunk for a pass of nq queries over C columns.  Each chunk
-// reads the tile's columns once (from L1/L2 after the first), so fewer
-// columns leave room for more queries per chunk.
-template <int C>
-constexpr int few_chunk_max() { return C <= 2 ? 8 : C <= 4 ? 4 : 2; }
+// Most queries per chunk over ncols columns.  Each chunk reads the tile's
+// columns once (from L1/L2 after the first), so fewer columns leave room
+// for more queries per chunk.
+constexpr int few_chunk_max(int ncols) { return ncols <= 2 ? 8 : ncols <= 4 ? 4 : 2; }
+// Queries per chunk for a pass of nq queries over ncols columns.
 inline int few_chunk(int nq, int ncols) {
-  const int q = ncols <= 2 ? 8 : ncols <= 4 ? 4 : 2;
+  const int q = few_chunk_max(ncols);
   return nq < q ? (nq <= 1 ? 1 : nq <= 2 ? 2 : q) : q;
 }
 
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kFewWarps * 32, 4) batch_few_kernel(const __gr
 
 template <int C>
 void launch_few(const FewPass &fp, int grid, cudaStream_t s) {
-  constexpr int Q = few_chunk_max<C>();
+  constexpr int Q = few_chunk_max(C);
   switch (few_chunk(fp.nq, C)) {
     case 1: batch_few_kernel<C, 1><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
     case 2: batch_few_kernel<C, 2><<<grid, kFewWarps * 32, 0, s>>>(fp); break;
