@@ -239,10 +239,11 @@ def test_batch_host_buffers(ctx, n, nq):
     assert ctx.nrows == 1000
 
 
-@pytest.mark.parametrize("nq", [7, 100, 400])
+@pytest.mark.parametrize("nq", [1, 7, 100, 200, 400])
 def test_prepared_batch_graph_replays_match(ctx, nq):
-    """Graph replays of each pass shape: term by term (7 queries), 128 slots
-    (100) and 512 slots (400), with queries outside the kernels."""
+    """Graph replays of each pass shape: a fused scan (1 query), term by term
+    (7), 128 slots (100), 256 slots (200) and 512 slots (400), with queries
+    outside the kernels."""
     n = 333_333
     cols = [D.uniform(n, 300), D.zipf(n, 301, 1.5), D.uniform(n, 302, 64)]
     ctx.load_columns(cols)
