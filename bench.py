@@ -454,6 +454,21 @@ def run(args):
                "h2d_bytes_per_step": int(4 * n * len(cols)), "d2h_bytes_per_step": int(nq * (stride * 4 + 8)),
                "queries_per_s": round(nq * world / e2e_s, 2), "ms_per_step": round(e2e_s * 1e3, 2),
                "api": "rts_scan_batch_host"}
+        # the box's own pinned device-to-host copy rate (the e2e step's floor:
+        # its bitmaps cannot leave the device faster)
+        m = min(out.numel(), hb.numel(), 1 << 29)
+        src, dst = out.view(-1)[:m], hb.view(-1)[:m]
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        d2h = 3 * 4 * m / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        e2e["pinned_d2h_GB_s"] = round(d2h, 2)
+        e2e["d2h_floor_ms"] = round(e2e["d2h_bytes_per_step"] / d2h / 1e6, 2)
         del hb, host_cols
 
     gbs_total = bytes_step * world / (ms_step * 1e-3) / 1e9
