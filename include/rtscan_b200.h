@@ -264,8 +264,9 @@ typedef struct rts_batch_config {
   int32_t variant;              /* 4 (default): passes of up to 512 queries over CTA-wide row
                                    blocks, each pass in the smallest of the 128-, 256- and
                                    512-slot shapes that holds it, passes of at most 20 queries
-                                   tested term by term and a pass of one query run as a fused
-                                   scan; 3: 256-query passes, one 256-row block per warp */
+                                   tested term by term, and passes of one query (or two or
+                                   three with at most six terms) run as one fused scan per
+                                   query; 3: 256-query passes, one 256-row block per warp */
   int32_t warps_per_cta;        /* variant 3: 8 or 16 (each warp stages 8 KiB of result words) */
   int32_t max_queries_per_pass; /* 1..512 (variant 4), 1..256 (variant 3) */
   uint32_t table_budget_bytes;  /* shared memory a pass may use for its mask tables: 4 KiB up to
