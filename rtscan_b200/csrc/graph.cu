@@ -50,7 +50,7 @@ rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t 
   p->ctx = ctx;
   cudaStream_t cap = nullptr;
   try {
-    RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms, offsets, nq);
     std::vector<int> inside, outside;
     for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);

@@ -281,6 +281,10 @@ struct rts_server {
     stop.store(true);
     cv_work.notify_all();
     if (worker.joinable()) worker.join();
+    // runs on the caller's thread (rts_server_stop, or a failed start):
+    // switch to the context's device and give the caller's back at the end
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
     cudaSetDevice(ctx->device);
     if (stream) cudaStreamSynchronize(stream);
     for (auto &b : pb) {
@@ -296,6 +300,7 @@ struct rts_server {
     if (counts) cudaFree(counts);
     if (stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
   }
 };
 
@@ -338,7 +343,7 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
     }
     if (c.segment_rows % 4096) throw rts::Error(RTS_ERR_ARG, "segment_rows must be a multiple of 4096");
     srv->cfg = c;
-    RTS_CUDA(cudaSetDevice(ctx->device));
+    rts::DeviceGuard device_guard(ctx->device);
     srv->nrows = ctx->nrows;
     srv->words = rts::words_for(ctx->nrows);
     srv->stride = (srv->words + 31) / 32 * 32;
