@@ -20,6 +20,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -95,18 +97,16 @@ struct ParsedLine {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-rts_status rts_parse_scan_cmd(const char *text, uint64_t len, int32_t ncols, rts_qset **out) {
-  if (!out || (!text && len) || ncols < 1) return rts::set_thread_error(RTS_ERR_ARG, "bad arguments");
-  *out = nullptr;
-  auto *qs = new (std::nothrow) rts_qset();
-  if (!qs) return RTS_ERR_NOMEM;
+rts_status parse_scan_cmd(const char *text, uint64_t len, int32_t ncols, rts_qset **out) {
+  std::unique_ptr<rts_qset> owner(new (std::nothrow) rts_qset());
+  if (!owner) return rts::set_thread_error(RTS_ERR_NOMEM, "scan_cmd: host allocation failed");
+  rts_qset *qs = owner.get();
   std::vector<ParsedLine> pending;
   uint64_t pos = 0;
   int lineno = 0;
   auto error = [&](const std::string &m) {
-    delete qs;
     return rts::set_thread_error(RTS_ERR_PARSE, "scan_cmd line " + std::to_string(lineno) + ": " + m);
   };
   while (pos < len) {
@@ -161,8 +161,22 @@ rts_status rts_parse_scan_cmd(const char *text, uint64_t len, int32_t ncols, rts
       pending.clear();
     }
   }
-  *out = qs;
+  *out = owner.release();
   return RTS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rts_status rts_parse_scan_cmd(const char *text, uint64_t len, int32_t ncols, rts_qset **out) {
+  if (!out || (!text && len) || ncols < 1) return rts::set_thread_error(RTS_ERR_ARG, "bad arguments");
+  *out = nullptr;
+  try {  // no exception crosses the C boundary
+    return parse_scan_cmd(text, len, ncols, out);
+  } catch (const std::bad_alloc &) {
+    return rts::set_thread_error(RTS_ERR_NOMEM, "scan_cmd: host allocation failed");
+  }
 }
 
 int32_t rts_qset_size(const rts_qset *qs) { return qs ? (int32_t)qs->queries.size() : 0; }
