@@ -30,6 +30,7 @@
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -311,6 +312,22 @@ rts_status fail(rts_server *srv, rts_status code, const std::string &m) {
   return rts::set_thread_error(code, m);
 }
 
+// Run a C-ABI body and turn an exception (a host allocation that failed, a
+// thread that could not start) into a status, so that none crosses the C
+// boundary.
+template <class F>
+rts_status srv_guarded(rts_server *srv, F &&f) {
+  try {
+    return f();
+  } catch (const rts::Error &e) {
+    return fail(srv, e.code, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(srv, RTS_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(srv, RTS_ERR_STATE, e.what());
+  }
+}
+
 double percentile(std::vector<double> v, double p) {
   if (v.empty()) return 0.0;
   std::sort(v.begin(), v.end());
@@ -369,170 +386,189 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
 }
 
 rts_status rts_server_submit(rts_server *srv, const rts_term *terms, int32_t nterms, uint64_t *ticket) {
-  if (!srv || !ticket || nterms < 0 || (nterms > 0 && !terms)) return fail(srv, RTS_ERR_ARG, "bad submit arguments");
-  for (int i = 0; i < nterms; i++)
-    if (terms[i].column < 0 || terms[i].column >= (int)srv->ctx->cols.size())
-      return fail(srv, RTS_ERR_ARG, "term column out of range");
-  const double t_submit = now_s();
-  std::lock_guard<std::mutex> lk(srv->mu);
-  if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
-  if ((int64_t)srv->queue.size() >= srv->cfg.max_queue) {
-    srv->rejected++;
-    return fail(srv, RTS_ERR_FULL, "request queue full");
-  }
-  Request r;
-  r.ticket = srv->next_ticket++;
-  r.terms.assign(terms, terms + nterms);
-  r.t_submit = t_submit;
-  *ticket = r.ticket;
-  srv->queue.push_back(std::move(r));
-  srv->submitted++;
-  srv->cv_work.notify_one();
-  return RTS_OK;
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv || !ticket || nterms < 0 || (nterms > 0 && !terms)) return fail(srv, RTS_ERR_ARG, "bad submit arguments");
+    for (int i = 0; i < nterms; i++)
+      if (terms[i].column < 0 || terms[i].column >= (int)srv->ctx->cols.size())
+        return fail(srv, RTS_ERR_ARG, "term column out of range");
+    const double t_submit = now_s();
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+    if ((int64_t)srv->queue.size() >= srv->cfg.max_queue) {
+      srv->rejected++;
+      return fail(srv, RTS_ERR_FULL, "request queue full");
+    }
+    Request r;
+    r.ticket = srv->next_ticket++;
+    r.terms.assign(terms, terms + nterms);
+    r.t_submit = t_submit;
+    *ticket = r.ticket;
+    srv->queue.push_back(std::move(r));
+    srv->submitted++;
+    srv->cv_work.notify_one();
+    return RTS_OK;
+  });
 }
 
 rts_status rts_server_poll(rts_server *srv, uint64_t ticket, int32_t *done, uint64_t *count) {
-  if (!srv || !done) return fail(srv, RTS_ERR_ARG, "bad poll arguments");
-  std::lock_guard<std::mutex> lk(srv->mu);
-  if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
-  *done = 0;
-  auto it = srv->ticket_slot.find(ticket);
-  if (it == srv->ticket_slot.end()) {
-    for (auto &r : srv->queue)
-      if (r.ticket == ticket) return RTS_OK;
-    return fail(srv, RTS_ERR_ARG, "unknown ticket");
-  }
-  rts_server::Slot &S = srv->slots[it->second];
-  if (S.state == DONE) {
-    *done = 1;
-    if (count) {
-      unsigned long long c = 0;
-      cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
-      cudaStreamSynchronize(srv->copy_stream);
-      *count = c;
-    }
-  }
-  return RTS_OK;
-}
-
-rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms, uint64_t *count) {
-  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
-  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
-  std::unique_lock<std::mutex> lk(srv->mu);
-  while (true) {
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv || !done) return fail(srv, RTS_ERR_ARG, "bad poll arguments");
+    std::lock_guard<std::mutex> lk(srv->mu);
     if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+    *done = 0;
     auto it = srv->ticket_slot.find(ticket);
-    if (it != srv->ticket_slot.end() && srv->slots[it->second].state == DONE) {
+    if (it == srv->ticket_slot.end()) {
+      for (auto &r : srv->queue)
+        if (r.ticket == ticket) return RTS_OK;
+      return fail(srv, RTS_ERR_ARG, "unknown ticket");
+    }
+    rts_server::Slot &S = srv->slots[it->second];
+    if (S.state == DONE) {
+      *done = 1;
       if (count) {
         unsigned long long c = 0;
         cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
         cudaStreamSynchronize(srv->copy_stream);
         *count = c;
       }
-      return RTS_OK;
     }
-    if (it == srv->ticket_slot.end()) {
-      bool queued = false;
-      for (auto &r : srv->queue) queued = queued || r.ticket == ticket;
-      if (!queued) return fail(srv, RTS_ERR_ARG, "unknown ticket");
+    return RTS_OK;
+  });
+}
+
+rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms, uint64_t *count) {
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+    std::unique_lock<std::mutex> lk(srv->mu);
+    while (true) {
+      if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
+      auto it = srv->ticket_slot.find(ticket);
+      if (it != srv->ticket_slot.end() && srv->slots[it->second].state == DONE) {
+        if (count) {
+          unsigned long long c = 0;
+          cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+          cudaStreamSynchronize(srv->copy_stream);
+          *count = c;
+        }
+        return RTS_OK;
+      }
+      if (it == srv->ticket_slot.end()) {
+        bool queued = false;
+        for (auto &r : srv->queue) queued = queued || r.ticket == ticket;
+        if (!queued) return fail(srv, RTS_ERR_ARG, "unknown ticket");
+      }
+      if (srv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+        auto it2 = srv->ticket_slot.find(ticket);
+        if (it2 != srv->ticket_slot.end() && srv->slots[it2->second].state == DONE) continue;
+        return fail(srv, RTS_ERR_TIMEOUT, "request not done within the timeout");
+      }
     }
-    if (srv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
-      auto it2 = srv->ticket_slot.find(ticket);
-      if (it2 != srv->ticket_slot.end() && srv->slots[it2->second].state == DONE) continue;
-      return fail(srv, RTS_ERR_TIMEOUT, "request not done within the timeout");
-    }
-  }
+  });
 }
 
 rts_status rts_server_fetch(rts_server *srv, uint64_t ticket, uint32_t *host_bitmap, uint64_t *count) {
-  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
-  std::lock_guard<std::mutex> lk(srv->mu);
-  auto it = srv->ticket_slot.find(ticket);
-  if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown or unfinished ticket");
-  const int sl = it->second;
-  rts_server::Slot &S = srv->slots[sl];
-  if (S.state != DONE) return fail(srv, RTS_ERR_STATE, "request not done");
-  cudaError_t e = cudaSuccess;
-  if (host_bitmap)
-    e = cudaMemcpyAsync(host_bitmap, srv->bitmaps + (uint64_t)sl * srv->stride, srv->words * 4,
-                        cudaMemcpyDeviceToHost, srv->copy_stream);
-  unsigned long long c = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&c, srv->counts + sl, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(srv->copy_stream);
-  if (e != cudaSuccess) return fail(srv, RTS_ERR_CUDA, std::string("fetch: ") + cudaGetErrorString(e));
-  if (count) *count = c;
-  S.state = FREE;
-  srv->ticket_slot.erase(it);
-  srv->free_slots.push_back(sl);
-  srv->cv_work.notify_one();
-  return RTS_OK;
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->ticket_slot.find(ticket);
+    if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown or unfinished ticket");
+    const int sl = it->second;
+    rts_server::Slot &S = srv->slots[sl];
+    if (S.state != DONE) return fail(srv, RTS_ERR_STATE, "request not done");
+    cudaError_t e = cudaSuccess;
+    if (host_bitmap)
+      e = cudaMemcpyAsync(host_bitmap, srv->bitmaps + (uint64_t)sl * srv->stride, srv->words * 4,
+                          cudaMemcpyDeviceToHost, srv->copy_stream);
+    unsigned long long c = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&c, srv->counts + sl, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(srv->copy_stream);
+    if (e != cudaSuccess) return fail(srv, RTS_ERR_CUDA, std::string("fetch: ") + cudaGetErrorString(e));
+    if (count) *count = c;
+    S.state = FREE;
+    srv->ticket_slot.erase(it);
+    srv->free_slots.push_back(sl);
+    srv->cv_work.notify_one();
+    return RTS_OK;
+  });
 }
 
 rts_status rts_server_cancel(rts_server *srv, uint64_t ticket) {
-  if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
-  std::lock_guard<std::mutex> lk(srv->mu);
-  for (auto it = srv->queue.begin(); it != srv->queue.end(); ++it)
-    if (it->ticket == ticket) {
-      srv->queue.erase(it);
-      srv->cancelled++;
-      return RTS_OK;
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    for (auto it = srv->queue.begin(); it != srv->queue.end(); ++it)
+      if (it->ticket == ticket) {
+        srv->queue.erase(it);
+        srv->cancelled++;
+        return RTS_OK;
+      }
+    auto it = srv->ticket_slot.find(ticket);
+    if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown ticket");
+    rts_server::Slot &S = srv->slots[it->second];
+    if (S.state == ACTIVE) {
+      // kernels already queued may still write this slot: free it after them
+      S.ev = srv->get_event();
+      cudaEventRecord(S.ev, srv->stream);
+      S.state = CANCELLING;
+      srv->active_version++;
+    } else if (S.state == FINISHING) {
+      S.state = CANCELLING;
+    } else if (S.state == DONE) {
+      S.state = FREE;
+      srv->free_slots.push_back(it->second);
     }
-  auto it = srv->ticket_slot.find(ticket);
-  if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown ticket");
-  rts_server::Slot &S = srv->slots[it->second];
-  if (S.state == ACTIVE) {
-    // kernels already queued may still write this slot: free it after them
-    S.ev = srv->get_event();
-    cudaEventRecord(S.ev, srv->stream);
-    S.state = CANCELLING;
-    srv->active_version++;
-  } else if (S.state == FINISHING) {
-    S.state = CANCELLING;
-  } else if (S.state == DONE) {
-    S.state = FREE;
-    srv->free_slots.push_back(it->second);
-  }
-  srv->ticket_slot.erase(it);
-  srv->cancelled++;
-  return RTS_OK;
+    srv->ticket_slot.erase(it);
+    srv->cancelled++;
+    return RTS_OK;
+  });
 }
 
 rts_status rts_server_get_stats(rts_server *srv, rts_server_stats *st) {
-  if (!srv || !st) return fail(srv, RTS_ERR_ARG, "null argument");
-  std::lock_guard<std::mutex> lk(srv->mu);
-  memset(st, 0, sizeof *st);
-  st->submitted = srv->submitted;
-  st->completed = srv->completed;
-  st->rejected = srv->rejected;
-  st->cancelled = srv->cancelled;
-  st->steps = srv->steps;
-  st->queued = srv->queue.size();
-  int active = 0;
-  for (auto &S : srv->slots) active += S.state == ACTIVE;
-  st->active = (uint32_t)active;
-  st->p50_ms = percentile(srv->latencies, 0.50) * 1e3;
-  st->p99_ms = percentile(srv->latencies, 0.99) * 1e3;
-  st->p999_ms = percentile(srv->latencies, 0.999) * 1e3;
-  double mx = 0, sum = 0;
-  for (double v : srv->latencies) {
-    mx = std::max(mx, v);
-    sum += v;
-  }
-  st->max_ms = mx * 1e3;
-  st->mean_ms = srv->latencies.empty() ? 0 : sum / (double)srv->latencies.size() * 1e3;
-  return RTS_OK;
+  return srv_guarded(srv, [&]() -> rts_status {
+    if (!srv || !st) return fail(srv, RTS_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    memset(st, 0, sizeof *st);
+    st->submitted = srv->submitted;
+    st->completed = srv->completed;
+    st->rejected = srv->rejected;
+    st->cancelled = srv->cancelled;
+    st->steps = srv->steps;
+    st->queued = srv->queue.size();
+    int active = 0;
+    for (auto &S : srv->slots) active += S.state == ACTIVE;
+    st->active = (uint32_t)active;
+    st->p50_ms = percentile(srv->latencies, 0.50) * 1e3;
+    st->p99_ms = percentile(srv->latencies, 0.99) * 1e3;
+    st->p999_ms = percentile(srv->latencies, 0.999) * 1e3;
+    double mx = 0, sum = 0;
+    for (double v : srv->latencies) {
+      mx = std::max(mx, v);
+      sum += v;
+    }
+    st->max_ms = mx * 1e3;
+    st->mean_ms = srv->latencies.empty() ? 0 : sum / (double)srv->latencies.size() * 1e3;
+    return RTS_OK;
+  });
 }
 
 rts_status rts_server_stop(rts_server *srv) {
   if (!srv) return RTS_OK;
-  std::string fatal;
-  {
+  bool had_fatal = false;
+  std::string msg;
+  try {
     std::lock_guard<std::mutex> lk(srv->mu);
-    fatal = srv->fatal;
+    had_fatal = !srv->fatal.empty();
+    if (had_fatal) msg = "server had stopped: " + srv->fatal;
+  } catch (const std::exception &) {
   }
-  delete srv;
-  if (!fatal.empty()) return rts::set_thread_error(RTS_ERR_CUDA, "server had stopped: " + fatal);
-  return RTS_OK;
+  delete srv;  // nothing below touches the server
+  if (!had_fatal) return RTS_OK;
+  try {
+    return rts::set_thread_error(RTS_ERR_CUDA, msg);
+  } catch (const std::exception &) {
+    return RTS_ERR_CUDA;
+  }
 }
 
 // Open-loop replay for benchmarks: request q is submitted at arrival_s[q]
@@ -541,86 +577,88 @@ rts_status rts_server_stop(rts_server *srv) {
 // the queue was full).  Blocks until every request is done.
 rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets, int32_t nq,
                              const double *arrival_s, double *latency_ms) {
-  rts::Range nvtx_range_("rts_server_replay");
-  if (!srv || nq < 0 || (nq > 0 && (!offsets || !arrival_s || !latency_ms)))
-    return fail(srv, RTS_ERR_ARG, "bad replay arguments");
-  std::unordered_map<uint64_t, int> index_of;  // ticket -> query, filled by the producer
-  std::vector<double> t_sub(nq, 0);
-  std::atomic<int> produced{0};
-  std::atomic<int> rejected{0};
-  rts_status prod_err = RTS_OK;
-  std::mutex map_mu;
-  {
-    std::lock_guard<std::mutex> lk(srv->mu);
-    srv->track_done = true;
-    srv->done_tickets.clear();
-  }
-  const double t0 = now_s();
-  std::thread producer([&] {
-    for (int q = 0; q < nq; q++) {
-      const double due = t0 + arrival_s[q];
-      while (now_s() < due) {
-        const double left = due - now_s();
-        if (left > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(left * 5e5)));
-      }
-      t_sub[q] = now_s();
-      uint64_t tk = 0;
-      std::lock_guard<std::mutex> ml(map_mu);  // the consumer may look the ticket up right away
-      const rts_status rc = rts_server_submit(srv, terms + offsets[q], offsets[q + 1] - offsets[q], &tk);
-      if (rc == RTS_ERR_FULL) {
-        latency_ms[q] = -1;
-        rejected++;
-      } else if (rc != RTS_OK) {
-        prod_err = rc;
-        produced.store(nq);
-        return;
-      } else {
-        index_of[tk] = q;
-      }
-      produced.store(q + 1);
-    }
-  });
-  // consumer: release every finished request as it completes
-  int finished = 0;
-  rts_status rc = RTS_OK;
-  while (rc == RTS_OK) {
-    std::vector<std::pair<uint64_t, double>> batch;
+  return srv_guarded(srv, [&]() -> rts_status {
+    rts::Range nvtx_range_("rts_server_replay");
+    if (!srv || nq < 0 || (nq > 0 && (!offsets || !arrival_s || !latency_ms)))
+      return fail(srv, RTS_ERR_ARG, "bad replay arguments");
+    std::unordered_map<uint64_t, int> index_of;  // ticket -> query, filled by the producer
+    std::vector<double> t_sub(nq, 0);
+    std::atomic<int> produced{0};
+    std::atomic<int> rejected{0};
+    rts_status prod_err = RTS_OK;
+    std::mutex map_mu;
     {
-      std::unique_lock<std::mutex> lk(srv->mu);
-      if (srv->done_tickets.empty()) srv->cv_done.wait_for(lk, std::chrono::milliseconds(1));
-      if (!srv->fatal.empty()) {
-        rc = RTS_ERR_CUDA;
-        break;
-      }
-      batch.swap(srv->done_tickets);
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->track_done = true;
+      srv->done_tickets.clear();
     }
-    for (auto &d : batch) {
-      int q;
+    const double t0 = now_s();
+    std::thread producer([&] {
+      for (int q = 0; q < nq; q++) {
+        const double due = t0 + arrival_s[q];
+        while (now_s() < due) {
+          const double left = due - now_s();
+          if (left > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(left * 5e5)));
+        }
+        t_sub[q] = now_s();
+        uint64_t tk = 0;
+        std::lock_guard<std::mutex> ml(map_mu);  // the consumer may look the ticket up right away
+        const rts_status rc = rts_server_submit(srv, terms + offsets[q], offsets[q + 1] - offsets[q], &tk);
+        if (rc == RTS_ERR_FULL) {
+          latency_ms[q] = -1;
+          rejected++;
+        } else if (rc != RTS_OK) {
+          prod_err = rc;
+          produced.store(nq);
+          return;
+        } else {
+          index_of[tk] = q;
+        }
+        produced.store(q + 1);
+      }
+    });
+    // consumer: release every finished request as it completes
+    int finished = 0;
+    rts_status rc = RTS_OK;
+    while (rc == RTS_OK) {
+      std::vector<std::pair<uint64_t, double>> batch;
       {
-        std::lock_guard<std::mutex> ml(map_mu);
-        auto it = index_of.find(d.first);
-        if (it == index_of.end()) continue;  // not one of this replay's requests
-        q = it->second;
-        index_of.erase(it);
+        std::unique_lock<std::mutex> lk(srv->mu);
+        if (srv->done_tickets.empty()) srv->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+        if (!srv->fatal.empty()) {
+          rc = RTS_ERR_CUDA;
+          break;
+        }
+        batch.swap(srv->done_tickets);
       }
-      rc = rts_server_fetch(srv, d.first, nullptr, nullptr);
-      if (rc != RTS_OK) break;
-      latency_ms[q] = (d.second - t_sub[q]) * 1e3;
-      finished++;
+      for (auto &d : batch) {
+        int q;
+        {
+          std::lock_guard<std::mutex> ml(map_mu);
+          auto it = index_of.find(d.first);
+          if (it == index_of.end()) continue;  // not one of this replay's requests
+          q = it->second;
+          index_of.erase(it);
+        }
+        rc = rts_server_fetch(srv, d.first, nullptr, nullptr);
+        if (rc != RTS_OK) break;
+        latency_ms[q] = (d.second - t_sub[q]) * 1e3;
+        finished++;
+      }
+      if (prod_err != RTS_OK) rc = prod_err;
+      if (produced.load() == nq && finished + rejected.load() == nq) break;
     }
-    if (prod_err != RTS_OK) rc = prod_err;
-    if (produced.load() == nq && finished + rejected.load() == nq) break;
-  }
-  producer.join();
-  {
-    std::lock_guard<std::mutex> lk(srv->mu);
-    srv->track_done = false;
-    srv->done_tickets.clear();
-  }
-  if (rc == RTS_OK) rc = prod_err;
-  if (rc != RTS_OK && rc != RTS_ERR_CUDA) return rc;
-  if (rc == RTS_ERR_CUDA) return fail(srv, rc, "server stopped: " + srv->fatal);
-  return RTS_OK;
+    producer.join();
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->track_done = false;
+      srv->done_tickets.clear();
+    }
+    if (rc == RTS_OK) rc = prod_err;
+    if (rc != RTS_OK && rc != RTS_ERR_CUDA) return rc;
+    if (rc == RTS_ERR_CUDA) return fail(srv, rc, "server stopped: " + srv->fatal);
+    return RTS_OK;
+  });
 }
 
 }  // extern "C"
