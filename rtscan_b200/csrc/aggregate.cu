@@ -326,9 +326,9 @@ void *agg_scratch(rts_ctx *ctx, size_t bytes) {
 }
 
 
-rts_status fail(rts_ctx *ctx, const Error &e) {
+rts_status fail(rts_ctx *ctx, const std::exception &e) {
   if (ctx) ctx->err = e.what();
-  return set_thread_error(e.code, e.what());
+  return set_thread_error(status_of(e), e.what());
 }
 
 }  // namespace
@@ -364,7 +364,7 @@ rts_status rts_bitmap_rows_async(rts_ctx *ctx, const uint32_t *dev_bitmap, uint6
     RTS_CUDA(cudaGetLastError());
     ctx->launches += 3;
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     return rts::fail(ctx, e);
   }
 }
@@ -390,7 +390,7 @@ rts_status rts_bitmap_sum_async(rts_ctx *ctx, const uint32_t *dev_bitmap, int32_
     RTS_CUDA(cudaGetLastError());
     ctx->launches += 1;
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     return rts::fail(ctx, e);
   }
 }
@@ -460,7 +460,7 @@ rts_status rts_scan_aggregate_async(rts_ctx *ctx, const rts_term *terms, int32_t
     RTS_CUDA(cudaGetLastError());
     ctx->launches += 1;
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     return rts::fail(ctx, e);
   }
 }

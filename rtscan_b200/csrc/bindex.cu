@@ -692,8 +692,8 @@ rts_status rts_bindex_filter_vector(rts_ctx *ctx, int32_t column, int32_t k, uin
     RTS_CUDA(cudaMemcpy(host_out, B.fv + (uint64_t)k * B.fv_stride, rts::words_for(B.n) * 4,
                         cudaMemcpyDeviceToHost));
     return RTS_OK;
-  } catch (const rts::Error &e) {
-    return rts::set_thread_error(e.code, e.what());
+  } catch (const std::exception &e) {
+    return rts::set_thread_error(rts::status_of(e), e.what());
   }
 }
 
@@ -709,9 +709,9 @@ rts_status rts_bindex_scan_async(rts_ctx *ctx, const rts_term *terms, int32_t nt
     rts::bindex_query(ctx, terms, nterms, dev_bitmap, reinterpret_cast<unsigned long long *>(dev_count),
                       (cudaStream_t)stream);
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     ctx->err = e.what();
-    return rts::set_thread_error(e.code, e.what());
+    return rts::set_thread_error(rts::status_of(e), e.what());
   }
 }
 

@@ -222,8 +222,8 @@ rts_status rts_bindex_file_info(const char *path, int32_t *K, uint64_t *nrows) {
     if (K) *K = (int32_t)h.K;
     if (nrows) *nrows = h.n;
     return RTS_OK;
-  } catch (const rts::Error &e) {
-    return rts::set_thread_error(e.code, e.what());
+  } catch (const std::exception &e) {
+    return rts::set_thread_error(rts::status_of(e), e.what());
   }
 }
 

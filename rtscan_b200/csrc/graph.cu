@@ -91,10 +91,10 @@ rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t 
     ctx->launches += p->kernels;
     *out = p;
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     if (cap) cudaStreamDestroy(cap);
     delete p;
-    return fail(ctx, e.code, e.what());
+    return fail(ctx, rts::status_of(e), e.what());
   }
 }
 

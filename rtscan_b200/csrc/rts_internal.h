@@ -8,6 +8,7 @@
 #include <atomic>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -72,6 +73,14 @@ struct DeviceGuard {
   DeviceGuard(const DeviceGuard &) = delete;
   DeviceGuard &operator=(const DeviceGuard &) = delete;
 };
+
+// Status of an exception caught at the C boundary: the code an rts::Error
+// carries, RTS_ERR_NOMEM for a failed host allocation, RTS_ERR_STATE else.
+inline rts_status status_of(const std::exception &e) {
+  if (const auto *r = dynamic_cast<const Error *>(&e)) return r->code;
+  if (dynamic_cast<const std::bad_alloc *>(&e)) return RTS_ERR_NOMEM;
+  return RTS_ERR_STATE;
+}
 
 // Record `msg` as the calling thread's last error (rts_last_error(NULL)).
 rts_status set_thread_error(rts_status code, const std::string &msg);

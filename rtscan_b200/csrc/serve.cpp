@@ -378,10 +378,10 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
     srv->worker = std::thread([srv] { srv->run(); });
     *out = srv;
     return RTS_OK;
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     delete srv;
     ctx->err = e.what();
-    return rts::set_thread_error(e.code, e.what());
+    return rts::set_thread_error(rts::status_of(e), e.what());
   }
 }
 

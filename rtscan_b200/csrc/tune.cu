@@ -170,11 +170,11 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
     ctx->batch_cfg = best;
     ctx->nrows = saved_n;
     cache_store(cache_path, key, best, best_ms);
-  } catch (const rts::Error &e) {
+  } catch (const std::exception &e) {
     ctx->nrows = saved_n;
     ctx->batch_cfg = saved_cfg;
     ctx->err = e.what();
-    rc = rts::set_thread_error(e.code, e.what());
+    rc = rts::set_thread_error(rts::status_of(e), e.what());
   }
   if (bm) cudaFree(bm);
   if (cnt) cudaFree(cnt);
