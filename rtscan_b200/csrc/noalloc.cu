@@ -53,12 +53,9 @@ DeviceSetup &setup_for(int dev) {
 
 bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
-}  // namespace
-
-extern "C" rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev_cols, int32_t ncols, uint64_t nrows,
-                                                      const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
-                                                      uint64_t *dev_count, void *stream) {
-  rts::Range nvtx_range_("rts_scan_separate_noalloc_async");
+rts_status scan_separate_noalloc(const uint32_t *const *dev_cols, int32_t ncols, uint64_t nrows,
+                                 const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap, uint64_t *dev_count,
+                                 void *stream) {
   using rts::set_thread_error;
   if (nrows > RTS_NOALLOC_MAX_ROWS)
     return set_thread_error(RTS_ERR_ARG, "nrows " + std::to_string(nrows) +
@@ -126,4 +123,17 @@ extern "C" rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_thread_error(RTS_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   return RTS_OK;
+}
+
+}  // namespace
+
+extern "C" rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev_cols, int32_t ncols, uint64_t nrows,
+                                                      const rts_term *terms, int32_t nterms, uint32_t *dev_bitmap,
+                                                      uint64_t *dev_count, void *stream) {
+  rts::Range nvtx_range_("rts_scan_separate_noalloc_async");
+  try {  // the checks and the plan use host memory only; a failed host allocation is a status
+    return scan_separate_noalloc(dev_cols, ncols, nrows, terms, nterms, dev_bitmap, dev_count, stream);
+  } catch (const std::exception &e) {
+    return rts::set_thread_error(rts::status_of(e), e.what());
+  }
 }
