@@ -201,24 +201,26 @@ const char *rts_version(void) { return "rtscan_b200 0.1 sm_100a"; }
 uint64_t rts_bitmap_words(uint64_t nrows) { return rts::words_for(nrows); }
 
 rts_status rts_lower_op(int32_t op, uint32_t t1, uint32_t t2, uint32_t *lo, uint32_t *hi, int32_t *nonempty) {
-  if (!lo || !hi || !nonempty) return fail(nullptr, RTS_ERR_ARG, "null output pointer");
-  *nonempty = 1;
-  switch (op) {
-    case RTS_OP_LT:
-      if (t1 == 0) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
-      *lo = 0; *hi = t1 - 1; return RTS_OK;
-    case RTS_OP_LE: *lo = 0; *hi = t1; return RTS_OK;
-    case RTS_OP_GT:
-      if (t1 == 0xFFFFFFFFu) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
-      *lo = t1 + 1; *hi = 0xFFFFFFFFu; return RTS_OK;
-    case RTS_OP_GE: *lo = t1; *hi = 0xFFFFFFFFu; return RTS_OK;
-    case RTS_OP_EQ: *lo = t1; *hi = t1; return RTS_OK;
-    case RTS_OP_BT:
-      if (t1 > t2) std::swap(t1, t2);
-      if ((uint64_t)t2 <= (uint64_t)t1 + 1) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
-      *lo = t1 + 1; *hi = t2 - 1; return RTS_OK;
-    default: return fail(nullptr, RTS_ERR_ARG, "unknown operator " + std::to_string(op));
-  }
+  return guarded(nullptr, [&]() -> rts_status {
+    if (!lo || !hi || !nonempty) return fail(nullptr, RTS_ERR_ARG, "null output pointer");
+    *nonempty = 1;
+    switch (op) {
+      case RTS_OP_LT:
+        if (t1 == 0) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
+        *lo = 0; *hi = t1 - 1; return RTS_OK;
+      case RTS_OP_LE: *lo = 0; *hi = t1; return RTS_OK;
+      case RTS_OP_GT:
+        if (t1 == 0xFFFFFFFFu) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
+        *lo = t1 + 1; *hi = 0xFFFFFFFFu; return RTS_OK;
+      case RTS_OP_GE: *lo = t1; *hi = 0xFFFFFFFFu; return RTS_OK;
+      case RTS_OP_EQ: *lo = t1; *hi = t1; return RTS_OK;
+      case RTS_OP_BT:
+        if (t1 > t2) std::swap(t1, t2);
+        if ((uint64_t)t2 <= (uint64_t)t1 + 1) { *nonempty = 0; *lo = 1; *hi = 0; return RTS_OK; }
+        *lo = t1 + 1; *hi = t2 - 1; return RTS_OK;
+      default: return fail(nullptr, RTS_ERR_ARG, "unknown operator " + std::to_string(op));
+    }
+  });
 }
 
 rts_status rts_open(int32_t device, rts_ctx **out) {

@@ -102,7 +102,13 @@ rts_status rts_batch_launch(rts_prepared *p, void *stream) {
   rts::Range nvtx_range_("rts_batch_launch");
   if (!p) return rts::set_thread_error(RTS_ERR_ARG, "null prepared batch");
   cudaError_t e = cudaGraphLaunch(p->exec, (cudaStream_t)stream);
-  if (e != cudaSuccess) return fail(p->ctx, RTS_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    try {
+      return fail(p->ctx, RTS_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+    } catch (const std::exception &) {  // no room for the message
+      return RTS_ERR_CUDA;
+    }
+  }
   p->ctx->launches += p->kernels;
   return RTS_OK;
 }
