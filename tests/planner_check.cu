@@ -1,0 +1,201 @@
+// CPU check of the batch planner (compiled and run by
+// tests/test_planner_cpu.py; no GPU needed).  It includes the planner's
+// translation unit, builds plans for seeded random batches on a context
+// that has column pointers but no device (planning reads the pointers and
+// the launch configuration only), and checks every plan:
+//   * every kernel query sits in exactly one pass, no other query in any;
+//   * pass sizes: term-by-term passes of at most kFewMaxQueries queries,
+//     table passes of more, in the smallest of the 128/256/512-slot shapes;
+//   * term-by-term passes carry each query's terms (always-true elsewhere);
+//   * table passes: boundaries sorted and distinct, bmin/bmax their ends,
+//     every mask bit of every used slot equal to the query's verdict on the
+//     interval, every bucket of the index bracketing the true position of
+//     the values it maps, and the pass fitting shared memory.
+// Usage: planner_check SEED TRIALS; exit status 0 when every check holds.
+#include "../rtscan_b200/csrc/batch.cu"
+
+#include <cstdio>
+#include <random>
+
+namespace {
+
+int g_fails = 0;
+uint64_t g_table_passes = 0, g_few_passes = 0, g_kernel_queries = 0, g_bits = 0;
+#define CHECK(cond, ...)                     \
+  do {                                       \
+    if (!(cond)) {                           \
+      std::fprintf(stderr, __VA_ARGS__);     \
+      std::fprintf(stderr, "\n");            \
+      if (++g_fails > 20) std::exit(1);      \
+    }                                        \
+  } while (0)
+
+constexpr uintptr_t kColStride = 0x100000;
+constexpr uint32_t kMax = 0xFFFFFFFFu;
+
+int column_of(const uint32_t *p) { return (int)((uintptr_t)p / kColStride) - 1; }
+
+// The normalized term of query q on table column col: (lo, hi), or the
+// whole domain when q does not constrain it.
+void term_on(const rts::NormQuery &q, int col, uint32_t *lo, uint32_t *hi) {
+  *lo = 0;
+  *hi = kMax;
+  for (size_t k = 0; k < q.cols.size(); k++)
+    if (q.cols[k] == col) {
+      *lo = q.lo[k];
+      *hi = q.hi[k];
+    }
+}
+
+void check_table_pass(const rts::BatchPlan &plan, const rts::BatchPlan::Pass &b, const std::vector<rts::NormQuery> &norm,
+                      std::vector<int> &seen, std::mt19937_64 &rng) {
+  const rts::BatchPass &bp = b.bp;
+  const uint32_t *blob = plan.blob.data() + b.off;
+  g_table_passes++;
+  const int G = b.groups;
+  const int32_t *slot = reinterpret_cast<const int32_t *>(blob + bp.slot_off);
+  int nq = 0;
+  for (int s = 0; s < 32 * G; s++) nq += slot[s] >= 0;
+  CHECK(G == 4 || G == 8 || G == 16, "table pass with %d groups", G);
+  CHECK(nq > rts::kFewMaxQueries, "table pass of %d queries", nq);
+  CHECK(rts::pass_groups(nq) == G, "%d queries in a %d-group pass", nq, G);
+  CHECK(rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G) <= 227 * 1024, "pass needs %zu bytes of shared memory",
+        rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G));
+  for (int s = 0; s < 32 * G; s++)
+    if (slot[s] >= 0) {
+      CHECK(slot[s] < (int)seen.size(), "slot maps to query %d", slot[s]);
+      if (slot[s] < (int)seen.size()) seen[slot[s]]++;
+    }
+  for (int c = 0; c < bp.ncols; c++) {
+    const int col = column_of(bp.col[c]);
+    const uint32_t m = bp.m[c];
+    const uint32_t *B = blob + bp.bnd_off[c];
+    const uint32_t *tab = blob + bp.tab_off[c];
+    for (uint32_t i = 1; i < m; i++) CHECK(B[i - 1] < B[i], "boundaries not increasing at %u", i);
+    if (m) {
+      CHECK(bp.bmin[c] == B[0] && bp.bmax[c] == B[m - 1], "bmin/bmax");
+      CHECK(B[0] >= 1, "boundary 0");
+    }
+    // mask bits: interval pos holds [B[pos-1], B[pos]); its first value stands for it
+    for (uint32_t pos = 0; pos <= m; pos++) {
+      const uint32_t v = pos == 0 ? 0u : B[pos - 1];
+      for (int s = 0; s < 32 * G; s++) {
+        if (slot[s] < 0) continue;
+        uint32_t lo, hi;
+        term_on(norm[slot[s]], col, &lo, &hi);
+        const bool want = lo <= v && v <= hi;
+        const bool got = (tab[(size_t)pos * G + (s >> 5)] >> (s & 31)) & 1u;
+        g_bits++;
+        CHECK(want == got, "column %d pos %u slot %d: bit %d, query [%u, %u] at %u", col, pos, s, got, lo, hi, v);
+      }
+    }
+    // bucket index: the bucket of x brackets #{B <= x}
+    if (m) {
+      const uint16_t *bk = reinterpret_cast<const uint16_t *>(blob + bp.bkt_off[c]);
+      std::vector<uint32_t> xs;
+      for (uint32_t i = 0; i < m; i++) {
+        xs.push_back(B[i]);
+        if (B[i] > 0) xs.push_back(B[i] - 1);
+        if (B[i] < kMax) xs.push_back(B[i] + 1);
+      }
+      std::uniform_int_distribution<uint64_t> any(bp.bmin[c], bp.bmax[c]);
+      for (int r = 0; r < 64; r++) xs.push_back((uint32_t)any(rng));
+      for (uint32_t x : xs) {
+        if (x < bp.bmin[c] || x >= bp.bmax[c]) continue;
+        const uint32_t v = x - bp.bmin[c];
+        const uint32_t k = bp.lgm[c] ? rts::bucket_of(v, bp.lgm[c]) : v >> bp.shift[c];
+        CHECK(k < bp.nbk[c], "column %d value %u in bucket %u of %u", col, x, k, bp.nbk[c]);
+        if (k >= bp.nbk[c]) continue;
+        const uint32_t P = (uint32_t)(std::upper_bound(B, B + m, x) - B);
+        CHECK(bk[k] <= P && P <= bk[k + 1], "column %d value %u: position %u outside bucket %u [%u, %u]", col, x, P, k,
+              bk[k], bk[k + 1]);
+      }
+    }
+  }
+}
+
+void check_few_pass(const rts::BatchPlan::Pass &b, const std::vector<rts::NormQuery> &norm, std::vector<int> &seen) {
+  const rts::FewPass &f = b.fp;
+  g_few_passes++;
+  CHECK(f.nq >= 1 && f.nq <= rts::kFewMaxQueries, "term-by-term pass of %d queries", f.nq);
+  for (int j = 0; j < f.nq; j++) {
+    const int q = f.slot_query[j];
+    CHECK(q >= 0 && q < (int)seen.size(), "few slot maps to query %d", q);
+    if (q < 0 || q >= (int)seen.size()) continue;
+    seen[q]++;
+    for (int c = 0; c < f.ncols; c++) {
+      uint32_t lo, hi;
+      term_on(norm[q], column_of(f.col[c]), &lo, &hi);
+      CHECK(f.term[j][c].x == lo && f.term[j][c].y == hi - lo, "few pass: query %d column %d term", q, c);
+    }
+  }
+}
+
+uint32_t draw_bound(std::mt19937_64 &rng, const std::vector<uint32_t> &pool) {
+  std::uniform_int_distribution<int> pick(0, 3);
+  if (pick(rng) == 0) return (uint32_t)rng();
+  return pool[std::uniform_int_distribution<size_t>(0, pool.size() - 1)(rng)];
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  const uint64_t seed = argc > 1 ? std::strtoull(argv[1], nullptr, 10) : 1;
+  const int trials = argc > 2 ? std::atoi(argv[2]) : 20;
+  std::mt19937_64 rng(seed);
+  const int counts[] = {1, 2, 3, 4, 20, 21, 32, 100, 128, 129, 200, 256, 257, 400, 512, 513, 700, 1100};
+  for (int t = 0; t < trials; t++) {
+    auto *ctx = new rts_ctx();  // never destroyed: it owns no device memory
+    const int ncols = 1 + (int)(rng() % 10);
+    for (int c = 0; c < ncols; c++) ctx->cols.push_back(reinterpret_cast<const uint32_t *>(kColStride * (c + 1)));
+    ctx->nrows = 1 << 20;
+    ctx->sm_count = 148;
+    const size_t budgets[] = {136 * 1024, 64 * 1024, 8 * 1024};
+    ctx->batch_cfg.table_budget = budgets[rng() % 3];
+    const int nq = rng() % 4 ? counts[rng() % (sizeof counts / sizeof counts[0])] : 1 + (int)(rng() % 1100);
+    // bounds from a small pool (shared boundaries, domain edges) and random values
+    std::vector<uint32_t> pool = {0, 1, 2, kMax - 1, kMax, 1u << 31};
+    for (int i = 0; i < 40; i++) pool.push_back((uint32_t)rng() >> (rng() % 32));
+    std::vector<rts_term> terms;
+    std::vector<int32_t> offsets = {0};
+    for (int q = 0; q < nq; q++) {
+      const int k = 1 + (int)(rng() % std::min(ncols, 9));
+      for (int i = 0; i < k; i++) {
+        rts_term tm;
+        tm.column = (int32_t)(rng() % ncols);
+        uint32_t a = draw_bound(rng, pool), b = draw_bound(rng, pool);
+        if (rng() % 8 && a > b) std::swap(a, b);  // now and then an empty term
+        tm.lo = a;
+        tm.hi = b;
+        terms.push_back(tm);
+      }
+      offsets.push_back((int32_t)terms.size());
+    }
+    std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms.data(), offsets.data(), nq);
+    std::vector<int> inside;
+    for (int q = 0; q < nq; q++)
+      if (rts::runs_in_kernel(norm[q])) inside.push_back(q);
+    g_kernel_queries += inside.size();
+    std::vector<int> seen(nq, 0);
+    if (!inside.empty()) {
+      rts::BatchPlanPtr plan = rts::make_batch_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget);
+      for (const auto &b : plan->passes) {
+        if (b.few) check_few_pass(b, norm, seen);
+        else check_table_pass(*plan, b, norm, seen, rng);
+      }
+    }
+    for (int q = 0; q < nq; q++) {
+      const int want = rts::runs_in_kernel(norm[q]) ? 1 : 0;
+      CHECK(seen[q] == want, "trial %d: query %d in %d passes (want %d)", t, q, seen[q], want);
+    }
+  }
+  if (g_fails) {
+    std::fprintf(stderr, "%d checks failed\n", g_fails);
+    return 1;
+  }
+  std::printf("planner ok: %d trials, seed %llu: %llu kernel queries, %llu table passes, %llu term-by-term passes, "
+              "%llu mask bits\n",
+              trials, (unsigned long long)seed, (unsigned long long)g_kernel_queries, (unsigned long long)g_table_passes,
+              (unsigned long long)g_few_passes, (unsigned long long)g_bits);
+  return 0;
+}

@@ -1,0 +1,41 @@
+"""The batch planner on the CPU: tests/planner_check.cu includes the
+planner's translation unit, plans seeded random batches (1-10 columns,
+query counts at every pass-routing edge, three table budgets, empty and
+merged terms) on a context without a device, and checks each plan's
+routing, mask bits, bucket index and shared-memory fit.  Compiled here with
+nvcc against the library's other objects (built by __graft_entry__.build)."""
+import glob
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    objs = [o for o in glob.glob(os.path.join(ROOT, "rtscan_b200", "_build", "*.o"))
+            if not o.endswith("batch.cu.o")]
+    if not os.path.exists(nvcc) or not objs:
+        pytest.skip("needs nvcc and the library's objects (run the build first)")
+    out = str(tmp_path_factory.mktemp("planner") / "planner_check")
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17",
+           "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr",
+           os.path.join(ROOT, "tests", "planner_check.cu"), *objs, "-lcuda", "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return out
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4, 5])
+def test_planner_invariants(harness, seed):
+    r = subprocess.run([harness, str(seed), "30"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    m = re.search(r"(\d+) kernel queries, (\d+) table passes, (\d+) term-by-term passes, (\d+) mask bits", r.stdout)
+    assert m, r.stdout
+    queries, tables, few, bits = (int(x) for x in m.groups())
+    assert queries > 1000 and tables > 0 and few > 0 and bits > 100_000, r.stdout
