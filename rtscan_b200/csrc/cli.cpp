@@ -82,12 +82,25 @@ int main(int argc, char **argv) {
       case 'q': max_queries = atoi(optarg); break;
       case 'y': read_queries = atoi(optarg) != 0; break;
       case 'g': range_queries = atoi(optarg) != 0; break;
-      default: fprintf(stderr, "Error: unknown option %c\n", (char)opt); return 2;
+      default: fprintf(stderr, "see -h for the options\n"); return 2;  // getopt named the bad option
     }
   }
   if (!data || ncols < 1) {
     fprintf(stderr, "need -f <column-file> and -b <ncols>\n");
     return 2;
+  }
+  // argument errors before any device work
+  if (strcmp(mode, "auto") && strcmp(mode, "scan") && strcmp(mode, "bindex") && strcmp(mode, "batch")) {
+    fprintf(stderr, "Error: unknown mode %s (auto, scan, bindex or batch)\n", mode);
+    return 2;
+  }
+  if (!read_queries && max_queries < 1) {
+    fprintf(stderr, "-y 0 needs -q <queries>\n");
+    return 2;
+  }
+  if (read_queries && access(cmd_path, R_OK) != 0) {
+    fprintf(stderr, "Fail to open scan_cmd file %s\n", cmd_path);
+    return 1;
   }
   rts_ctx *ctx = nullptr;
   if (rts_open(device, &ctx) != RTS_OK) return die(nullptr, "open");
@@ -133,11 +146,7 @@ int main(int argc, char **argv) {
     size_t r;
     while ((r = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, r);
     fclose(fp);
-  } else {
-    if (max_queries < 1) {
-      fprintf(stderr, "-y 0 needs -q <queries>\n");
-      return 2;
-    }
+  } else {  // max_queries >= 1, checked above
     const uint32_t span = 0xFFFFFFFFu / (uint32_t)(max_queries + 1);
     for (int i = 0; i < max_queries; i++)
       for (int c = 0; c < ncols; c++)
