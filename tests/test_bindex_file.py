@@ -66,3 +66,40 @@ def test_file_info_missing_and_truncated(tmp_path):
     with pytest.raises(R.RtsError) as e:
         R.bindex_file_info(str(p))
     assert e.value.code == -5
+
+
+def test_every_single_bit_flip_is_refused(tmp_path):
+    """The header checksum covers every byte: flipping any one bit of a valid
+    header (fields, magic or the checksum itself) is a parse error."""
+    good = header(K=64, n=77_777)
+    p = tmp_path / "f.bdx"
+    for i in range(len(good)):
+        for bit in (0, 3, 7):
+            p.write_bytes(good[:i] + bytes([good[i] ^ (1 << bit)]) + good[i + 1:])
+            with pytest.raises(R.RtsError) as e:
+                R.bindex_file_info(str(p))
+            assert e.value.code == -5, (i, bit)
+
+
+hypothesis = pytest.importorskip("hypothesis")
+from hypothesis import given, settings, strategies as st  # noqa: E402
+
+
+@settings(max_examples=200, deadline=None)
+@given(data=st.one_of(
+    st.binary(max_size=300),
+    # well-formed headers (valid checksum) with arbitrary field values
+    st.builds(lambda K, n, s, ns, pl: header(K=K, n=n, fv_stride=s, nsample=ns, payload=pl),
+              st.integers(0, 1 << 20), st.integers(0, 1 << 40), st.integers(0, 1 << 40),
+              st.integers(0, 1 << 32), st.integers(0, (1 << 64) - 1))))
+def test_any_header_is_read_or_refused(tmp_path_factory, data):
+    p = tmp_path_factory.mktemp("fz") / "x.bdx"
+    p.write_bytes(data)
+    try:
+        K, n = R.bindex_file_info(str(p))
+    except R.RtsError as e:
+        assert e.code in (-4, -5), (e.code, data[:32])
+        return
+    # accepted: the fields it reports are the header's
+    k2, n2 = struct.unpack("<IQ", data[12:16] + data[16:24])
+    assert (K, n) == (k2, n2)
