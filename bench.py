@@ -69,8 +69,8 @@ def dist_env():
 # traffic-to-bytes ratio (the kernel streams each column once per launch and
 # writes each bitmap once, so its traffic grows in proportion).
 NCU_TRAFFIC = {
-    "batched": {"kernel": "batch4_kernel<4>", "capture": "3e7 rows x 4 columns, 512 queries, one launch",
-                "bytes": 480.2e6 + 1863.4e6, "launch_bytes": 4 * 4 * 3e7 + 512 * 3e7 / 8},
+    "batched": {"kernel": "batch4_kernel<4,16>", "capture": "3e7 rows x 4 columns, 512 queries, one launch",
+                "bytes": 480.4e6 + 1863.3e6, "launch_bytes": 4 * 4 * 3e7 + 512 * 3e7 / 8},
     "single": {"kernel": "scan_fused_kernel<1,1>", "capture": "1e8 rows x 1 column, one launch",
                "bytes": 408.9e6, "launch_bytes": 4 * 1e8 + 1e8 / 8},
 }
