@@ -585,7 +585,7 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
     std::vector<double> t_sub(nq, 0);
     std::atomic<int> produced{0};
     std::atomic<int> rejected{0};
-    rts_status prod_err = RTS_OK;
+    std::atomic<rts_status> prod_err{RTS_OK};  // written by the producer, read by the consumer
     std::mutex map_mu;
     {
       std::lock_guard<std::mutex> lk(srv->mu);
@@ -594,29 +594,41 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
     }
     const double t0 = now_s();
     std::thread producer([&] {
-      for (int q = 0; q < nq; q++) {
-        const double due = t0 + arrival_s[q];
-        while (now_s() < due) {
-          const double left = due - now_s();
-          if (left > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(left * 5e5)));
+      try {
+        for (int q = 0; q < nq; q++) {
+          const double due = t0 + arrival_s[q];
+          while (now_s() < due) {
+            const double left = due - now_s();
+            if (left > 2e-4) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)(left * 5e5)));
+          }
+          t_sub[q] = now_s();
+          uint64_t tk = 0;
+          std::lock_guard<std::mutex> ml(map_mu);  // the consumer may look the ticket up right away
+          const rts_status rc = rts_server_submit(srv, terms + offsets[q], offsets[q + 1] - offsets[q], &tk);
+          if (rc == RTS_ERR_FULL) {
+            latency_ms[q] = -1;
+            rejected++;
+          } else if (rc != RTS_OK) {
+            prod_err.store(rc);
+            produced.store(nq);
+            return;
+          } else {
+            index_of[tk] = q;
+          }
+          produced.store(q + 1);
         }
-        t_sub[q] = now_s();
-        uint64_t tk = 0;
-        std::lock_guard<std::mutex> ml(map_mu);  // the consumer may look the ticket up right away
-        const rts_status rc = rts_server_submit(srv, terms + offsets[q], offsets[q + 1] - offsets[q], &tk);
-        if (rc == RTS_ERR_FULL) {
-          latency_ms[q] = -1;
-          rejected++;
-        } else if (rc != RTS_OK) {
-          prod_err = rc;
-          produced.store(nq);
-          return;
-        } else {
-          index_of[tk] = q;
-        }
-        produced.store(q + 1);
+      } catch (const std::exception &) {  // no exception may leave the thread
+        prod_err.store(RTS_ERR_NOMEM);
+        produced.store(nq);
       }
     });
+    // join the producer on every way out, before the state it uses goes away
+    struct Joiner {
+      std::thread &t;
+      ~Joiner() {
+        if (t.joinable()) t.join();
+      }
+    } join_producer{producer};
     // consumer: release every finished request as it completes
     int finished = 0;
     rts_status rc = RTS_OK;
@@ -645,7 +657,7 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
         latency_ms[q] = (d.second - t_sub[q]) * 1e3;
         finished++;
       }
-      if (prod_err != RTS_OK) rc = prod_err;
+      if (prod_err.load() != RTS_OK) rc = prod_err.load();
       if (produced.load() == nq && finished + rejected.load() == nq) break;
     }
     producer.join();
@@ -654,7 +666,7 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
       srv->track_done = false;
       srv->done_tickets.clear();
     }
-    if (rc == RTS_OK) rc = prod_err;
+    if (rc == RTS_OK) rc = prod_err.load();
     if (rc != RTS_OK && rc != RTS_ERR_CUDA) return rc;
     if (rc == RTS_ERR_CUDA) return fail(srv, rc, "server stopped: " + srv->fatal);
     return RTS_OK;
