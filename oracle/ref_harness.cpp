@@ -17,8 +17,11 @@
 //
 // usage: ref_bindex_<N> -f <column file> -b <ncols> -p <scan_cmd>
 //                       [-o <out dir>] [-r <repeats>] [-n <max queries>]
+//                       [-c <checked queries>]
+// -c k runs the scalar-filter check on the first k queries only (default:
+// every query); a query left unchecked reports raw_hits -1 and equal -1.
 // stdout, one line per query:
-//   query <i> bindex_hits <a> raw_hits <b> equal <0|1> scan_ms <t>
+//   query <i> bindex_hits <a> raw_hits <b> equal <0|1|-1> scan_ms <t>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -92,9 +95,9 @@ static void run_op(BinDex *b, BITS *bm, const std::string &cmd, CODE t1, CODE t2
 
 int main(int argc, char **argv) {
   char path[4096] = "", cmd_path[4096] = "", out_dir[4096] = "";
-  int ncols = 1, repeats = 1, max_queries = 1 << 30;
+  int ncols = 1, repeats = 1, max_queries = 1 << 30, checked = 1 << 30;
   int opt;
-  while ((opt = getopt(argc, argv, "f:b:p:o:r:n:")) != -1) {
+  while ((opt = getopt(argc, argv, "f:b:p:o:r:n:c:")) != -1) {
     switch (opt) {
       case 'f': snprintf(path, sizeof path, "%s", optarg); break;
       case 'b': ncols = atoi(optarg); break;
@@ -102,11 +105,13 @@ int main(int argc, char **argv) {
       case 'o': snprintf(out_dir, sizeof out_dir, "%s", optarg); break;
       case 'r': repeats = atoi(optarg); break;
       case 'n': max_queries = atoi(optarg); break;
+      case 'c': checked = atoi(optarg); break;
       default: fprintf(stderr, "unknown option\n"); return 2;
     }
   }
   if (!path[0] || !cmd_path[0] || ncols < 1 || repeats < 1) {
-    fprintf(stderr, "usage: %s -f data -b ncols -p scan_cmd [-o dir] [-r repeats] [-n max_queries]\n", argv[0]);
+    fprintf(stderr, "usage: %s -f data -b ncols -p scan_cmd [-o dir] [-r repeats] [-n max_queries] [-c checked]\n",
+            argv[0]);
     return 2;
   }
   FILE *fp = fopen(path, "rb");
@@ -169,25 +174,32 @@ int main(int argc, char **argv) {
       if (ms < best) best = ms;
     }
 
-    for (int c = 0; c < ncols; c++) memset(chk[c], 0, bytes);
-    for (int c = 0; c < ncols; c++)
-      raw_scan_entry(&tl[c], &tr[c], cmd[c], bindexs[c], chk[c], chk[0], data[c]);
-
-    uint64_t a = count_bits(bm[0], kN), b = count_bits(chk[0], kN);
-    int equal = 1;
-    for (int i = 0; i < kN && equal; i++)
-      if (((bm[0][i >> 5] ^ chk[0][i >> 5]) >> (31 - (i & 31))) & 1u) equal = 0;
-    printf("query %d bindex_hits %llu raw_hits %llu equal %d scan_ms %.4f\n", q, (unsigned long long)a,
-           (unsigned long long)b, equal, best);
+    const bool check = q < checked;
+    uint64_t a = count_bits(bm[0], kN);
+    long long b = -1;
+    int equal = -1;
+    if (check) {
+      for (int c = 0; c < ncols; c++) memset(chk[c], 0, bytes);
+      for (int c = 0; c < ncols; c++)
+        raw_scan_entry(&tl[c], &tr[c], cmd[c], bindexs[c], chk[c], chk[0], data[c]);
+      b = (long long)count_bits(chk[0], kN);
+      equal = 1;
+      for (int i = 0; i < kN && equal; i++)
+        if (((bm[0][i >> 5] ^ chk[0][i >> 5]) >> (31 - (i & 31))) & 1u) equal = 0;
+    }
+    printf("query %d bindex_hits %llu raw_hits %lld equal %d scan_ms %.4f\n", q, (unsigned long long)a, b, equal,
+           best);
     fflush(stdout);
     if (out_dir[0]) {
       char fn[8192];
       snprintf(fn, sizeof fn, "%s/q%05d_bindex.bin", out_dir, q);
       FILE *o = fopen(fn, "wb");
       if (o) { fwrite(bm[0], sizeof(BITS), W, o); fclose(o); }
-      snprintf(fn, sizeof fn, "%s/q%05d_raw.bin", out_dir, q);
-      o = fopen(fn, "wb");
-      if (o) { fwrite(chk[0], sizeof(BITS), W, o); fclose(o); }
+      if (check) {
+        snprintf(fn, sizeof fn, "%s/q%05d_raw.bin", out_dir, q);
+        o = fopen(fn, "wb");
+        if (o) { fwrite(chk[0], sizeof(BITS), W, o); fclose(o); }
+      }
     }
   }
   return 0;

@@ -34,6 +34,7 @@ from rtscan_b200 import datagen as D  # noqa: E402
 
 N = 1 << 20           # compile-time row count of the harness (DATA_N)
 N_ODD = 1_000_003     # a row count that is not a multiple of 32
+N_C1 = 1 << 24        # the plain single-column scan at its own size
 
 
 def sha(a: np.ndarray) -> str:
@@ -104,6 +105,12 @@ def cases():
         lines += [f"lt {t}", f"ge {t}"]
     lines += ["bt 100 900", "eq 7", "le 0"]
     out.append(("uniform1000_odd_1c", N_ODD, [("uniform1000", 500)], lines))
+    # the plain single-column scan at its own size: 2^24 rows uniform on
+    # [0, 2^32) from default_rng(42), the 10 % range [q45, q55] of the data
+    # written as the reference's exclusive `bt` (1,677,722 rows), plus one
+    # 10 % range at each end of the domain
+    out.append(("c1_uniform32_2p24_1c", N_C1, [("uniform", 42)],
+                ["bt 1932185501 2361592940", "lt 429496730", "ge 3865470566"]))
     return out
 
 
@@ -118,7 +125,7 @@ def run_case(harness_dir, name, n, specs, lines):
     ncols = len(cols)
     binary = os.path.join(harness_dir, f"ref_bindex_{n}")
     if not os.access(binary, os.X_OK):
-        raise SystemExit(f"missing {binary}: make -C oracle ref REF=<reference> REF_NS='{N} {N_ODD}'")
+        raise SystemExit(f"missing {binary}: make -C oracle ref REF=<reference> REF_NS='{N} {N_ODD} {N_C1}'")
     with tempfile.TemporaryDirectory() as td:
         data = os.path.join(td, "cols.bin")
         D.write_columns(data, cols)

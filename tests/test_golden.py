@@ -89,3 +89,15 @@ def test_golden_covers_the_reference_edges():
     2^32-1, bindex.cpp:1419-1427); nothing else may differ."""
     bad = [(c["name"], q["lines"]) for c in CASES for q in c["queries"] if not q["bindex_equal"]]
     assert sorted(l[0] for _, l in bad) == ["gt 4294967295", "le 4294967295"]
+
+
+def test_c1_is_pinned_at_its_own_size():
+    """The plain single-column scan's own configuration (2^24 uniform rows
+    from default_rng(42), `bt 1932185501 2361592940`) is a golden case with
+    the count the reference reports for it."""
+    c1 = [c for c in CASES if c["name"] == "c1_uniform32_2p24_1c"]
+    assert len(c1) == 1 and c1[0]["n"] == 1 << 24
+    assert c1[0]["columns"] == [{"kind": "uniform", "seed": 42, "sha": c1[0]["columns"][0]["sha"]}]
+    q = c1[0]["queries"][0]
+    assert q["lines"] == ["bt 1932185501 2361592940"]
+    assert q["raw_hits"] == q["bindex_hits"] == 1_677_722
