@@ -21,11 +21,23 @@ Workloads (seeded synthetic data generated on the device; no dataset is read):
            Compared with the scan followed by the masked sum, and with the
            compaction of its bitmap to row ids.
 
-Under torchrun each rank scans its own rows (weak scaling, no collective on
-the data path); `value` is the aggregate over ranks.  Timing: W warm-up
-steps, then K steps between CUDA events on the launching stream, barrier +
-synchronize on both sides, max over ranks.  Inputs are larger than L2
-(400 MB per column).
+The default batched line also carries the other configurations of the
+scan, each timed with CUDA events on the launching stream beside its own
+roofline fraction: `single_1e8` (the plain one-column 1e8-row scan at 10 %),
+`sweep_1e8` (one-column queries at 0.1-90 % selectivity on a uniform 2^32
+column and on 2^8- and 2^6-value columns, fused scan and BinDex) and
+`multi_1e8` (2-, 3- and 4-column conjunctions, fused against separate
+per-column passes plus AND).
+
+`--gpus N` runs N ranks, one per GPU: under torchrun (WORLD_SIZE set) it
+must equal the world size; without it, bench.py starts itself under
+torch.distributed.run with N processes.  Each rank scans its own rows
+(weak scaling, no collective on the data path) and answers the same
+queries (rank 0's, broadcast); `value` is the aggregate over ranks and the
+counts of the first query are summed over ranks with one all-reduce.
+Timing: W warm-up steps, then K steps between CUDA events on the launching
+stream, barrier + synchronize on both sides, max over ranks.  Inputs are
+larger than L2 (400 MB per column).
 """
 from __future__ import annotations
 
@@ -60,6 +72,57 @@ Q6_TERMS = [(0, 19940101, 19950100), (1, 5, 7), (2, 0, 23)]
 def dist_env():
     return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
         int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def free_port():
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def launch_command(gpus, argv):
+    """The torch.distributed.run command that runs this script as `gpus`
+    ranks on one node (rendezvous on 127.0.0.1)."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+            "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)] + list(argv)
+
+
+def check_world(gpus):
+    """None when this process is the run itself; else the command that
+    starts `gpus` ranks.  A world size that disagrees with --gpus is an
+    error, so that a line never reports fewer GPUs than were asked for."""
+    if "WORLD_SIZE" in os.environ:
+        world = int(os.environ["WORLD_SIZE"])
+        if world != gpus:
+            raise SystemExit(f"bench.py: --gpus {gpus} but WORLD_SIZE={world}")
+        return None
+    return launch_command(gpus, sys.argv[1:]) if gpus > 1 else None
+
+
+def agree_queries(queries, world):
+    """Rank 0's queries on every rank (one broadcast): all ranks answer the
+    same queries on their own rows."""
+    if world == 1:
+        return queries
+    import torch.distributed as dist
+    box = [queries]
+    dist.broadcast_object_list(box, src=0)
+    return [[(int(c), int(lo), int(hi)) for c, lo, hi in q] for q in box[0]]
+
+
+def host_info():
+    """Host cores and CPU model of this machine (for the CPU baselines)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"host_cpus": os.cpu_count(), "cpu_model": model}
 
 
 # DRAM traffic of the dominant kernel from one ncu capture each
@@ -231,37 +294,49 @@ def step_bytes(n, queries):
 # the reference sources) when present, else the oracle's C restatement.
 # ----------------------------------------------------------------------------
 
-REF_N = 1 << 24
+REF_N = 1 << 24      # rows of the CPU sample in the GPU arm's cpu_baseline
+REF_THREADS = 20     # the reference's thread count (THREAD_NUM, bindex.cpp:27)
 
 
-def reference_binary():
-    p = os.path.join(ROOT, "oracle", "_ref", f"ref_bindex_{REF_N}")
+def reference_binary(n=REF_N):
+    p = os.path.join(ROOT, "oracle", "_ref", f"ref_bindex_{n}")
     return p if os.access(p, os.X_OK) else None
 
 
-def cpu_reference_run(cols_np, queries, repeats=3, max_seconds=60.0):
-    """Time the reference BinDex query loop (index build excluded) on
-    REF_N-row columns; returns (seconds per query, kind, cores, detail)."""
+def run_reference_harness(binary, cols_np, queries, checked=1, repeats=1, timeout=1800):
+    """The reference's own CPU path once over `queries`: its BinDex build of
+    every column, then its query loop (sieve + refine + AND merge per
+    query, timed per query like the reference's timer 11).  The scalar
+    filter checks the first `checked` queries.  Returns (build_ms, [scan_ms
+    per query], [bindex == scalar for the checked queries])."""
     from rtscan_b200 import datagen as D
-    ncols = len(cols_np)
-    binary = reference_binary()
+    with tempfile.TemporaryDirectory() as td:
+        data = os.path.join(td, "cols.bin")
+        D.write_columns(data, cols_np)
+        cmdf = os.path.join(td, "cmd.txt")
+        with open(cmdf, "w") as f:
+            f.write(D.to_scan_cmd(queries, len(cols_np)))
+        r = subprocess.run([binary, "-f", data, "-b", str(len(cols_np)), "-p", cmdf, "-r", str(repeats),
+                            "-c", str(checked)], capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError("reference harness failed: " + r.stderr[-500:])
+    build_ms = next(float(l.split()[1]) for l in r.stdout.splitlines() if l.startswith("build_ms"))
+    q = [l.split() for l in r.stdout.splitlines() if l.startswith("query ")]
+    if len(q) != len(queries):
+        raise RuntimeError(f"reference harness answered {len(q)} of {len(queries)} queries")
+    return build_ms, [float(x[-1]) for x in q], [x[7] == "1" for x in q if x[7] != "-1"]
+
+
+def cpu_reference_run(cols_np, queries, max_seconds=60.0):
+    """Seconds per query of the reference BinDex query loop (index build
+    excluded) on REF_N-row columns; returns (seconds, kind, cores, detail)."""
+    binary = reference_binary(len(cols_np[0]))
     if binary:
-        with tempfile.TemporaryDirectory() as td:
-            data = os.path.join(td, "cols.bin")
-            D.write_columns(data, cols_np)
-            cmdf = os.path.join(td, "cmd.txt")
-            with open(cmdf, "w") as f:
-                f.write(D.to_scan_cmd(queries, ncols))
-            t0 = time.time()
-            r = subprocess.run([binary, "-f", data, "-b", str(ncols), "-p", cmdf, "-r", str(repeats)],
-                               capture_output=True, text=True, timeout=max_seconds + 300)
-            if r.returncode != 0:
-                raise RuntimeError("reference harness failed: " + r.stderr[-500:])
-            q = [l.split() for l in r.stdout.splitlines() if l.startswith("query ")]
-            ms = [float(x[-1]) for x in q]
-            return (sum(ms) / 1e3 / len(ms), "reference", 20,
-                    {"queries": len(ms), "reference_bindex_equals_scalar": all(x[7] == "1" for x in q),
-                     "wall_s": round(time.time() - t0, 1)})
+        t0 = time.time()
+        build_ms, ms, eq = run_reference_harness(binary, cols_np, queries, checked=1, repeats=3)
+        return (sum(ms) / 1e3 / len(ms), "reference", REF_THREADS,
+                {"queries": len(ms), "reference_bindex_equals_scalar": all(eq), "index_build_ms": round(build_ms),
+                 "wall_s": round(time.time() - t0, 1)})
     from oracle import oracle as O
     t0 = time.time()
     done = 0
@@ -319,7 +394,12 @@ def run(args):
     world, rank, local = dist_env()
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # NCCL's communicator log shows the ranks of a scaling run
+        os.environ.setdefault("NCCL_DEBUG", "INFO")
+        os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = R.Context(local)
@@ -333,7 +413,10 @@ def run(args):
     cols = [gpu_column(torch, k, n, 1000 * (rank + 1) + i, dev) for i, k in enumerate(kinds)]
     ctx.attach_columns([c.data_ptr() for c in cols], n)
     samples = [host_sample(torch, c, seed=7 + i) for i, c in enumerate(cols)]
-    queries = make_queries(D, wl, samples, args.queries)
+    # host copy of the first rows of every column: the CPU baseline's sample
+    cpu_cols = [c[:min(REF_N, n)].cpu().numpy().view(np.uint32).copy() for c in cols] \
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and wl != "q6" else None
+    queries = agree_queries(make_queries(D, wl, samples, args.queries), world)
     pq = R.prepare(queries)
     nq = len(queries)
     words = R.bitmap_words(n)
@@ -429,6 +512,14 @@ def run(args):
                               "one_per_launch_qps": round(256 / (me4 * 1e-3), 1),
                               "speedup": round(me4 / mb4, 2)}
 
+    if wl == "batched" and not args.no_legs:
+        lclk = ClockSampler(local)
+        lclk.start()
+        extra["single_1e8"] = single_leg(torch, R, D, dev, args.nrows, hbm_peak)
+        extra["multi_1e8"] = multi_leg(torch, R, D, dev, args.nrows, hbm_peak)
+        extra["sweep_1e8"] = sweep_leg(torch, R, D, dev, args.nrows, hbm_peak)
+        extra["legs_clocks"] = lclk.stop()
+
     # e2e through the C-ABI with host buffers: the step's columns uploaded
     # from pinned host memory and every result bitmap + count read back.
     e2e = None
@@ -505,7 +596,7 @@ def run(args):
     if args.bindex_io and rank == 0:
         line["bindex_io"] = bindex_io_leg(torch, R, dev, args.bindex_io)
     if args.bindex_query and rank == 0:
-        line["bindex_query"] = bindex_query_leg(torch, R, D, dev, args.bindex_query)
+        line["bindex_query"] = sweep_leg(torch, R, D, dev, args.bindex_query, hbm_peak)
 
     if wl == "batched" and args.pass_sweep:
         line["pass_sweep"] = pass_sweep(torch, R, D, dev, rank, args.pass_sweep)
@@ -526,19 +617,21 @@ def run(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline and wl == "q6":
         line["cpu_baseline"] = q6_cpu_port(kinds, queries[0])
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cols_np = cpu_sample_columns(kinds, REF_N)
-        smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols_np]
-        qs = make_queries(D, wl, smp, args.queries)[: 16]
+        m = min(REF_N, n)
+        cols_np = cpu_cols
+        qs = queries[:16]
         sec, kind, cores, detail = cpu_reference_run(cols_np, qs)
         bprq = row_query_bytes(n, queries)
-        line["cpu_baseline"] = {"value": round(REF_N * bprq / sec / 1e9, 3), "unit": "GB/s", "cores": cores,
-                                "kind": kind, "queries_per_s": round(REF_N / n / sec, 3),
+        line["cpu_baseline"] = {"value": round(m * bprq / sec / 1e9, 3), "unit": "GB/s", "cores": cores,
+                                "kind": kind, "queries_per_s": round(m / n / sec, 3),
                                 "queries_per_s_sample": round(1.0 / sec, 2),
-                                "sample": f"{REF_N} rows x {len(cols_np)} columns, {len(qs)} queries of this "
-                                          "workload (reference BinDex query loop, index build excluded); "
-                                          f"credited {bprq:.4f} B per row and query, the workload's bytes "
-                                          "share; queries_per_s scaled to the workload's rows",
-                                **detail}
+                                "sample": f"the first {m} rows of this workload's {len(cols_np)} columns and its "
+                                          f"first {len(qs)} queries (reference BinDex query loop, "
+                                          f"{cores} threads, index build excluded); credited {bprq:.4f} B per "
+                                          "row and query, the workload's bytes share; queries_per_s scaled "
+                                          "to the workload's rows (the full-size reference run is "
+                                          "`--impl reference`)",
+                                **host_info(), **detail}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -574,44 +667,123 @@ def bindex_io_leg(torch, R, dev, n, K=128):
             "load_GB_s": round(size / load_s / 1e9, 2)}
 
 
-def bindex_query_leg(torch, R, D, dev, n, K=128):
-    """Single-column queries through the BinDex against fused scans of the
-    same queries, on a uniform column at 0.1/1/10/50/90 % selectivity and on
-    a column of 256 values (the single-column sweep's shapes): CUDA-event
-    medians on one stream, and each BinDex bitmap checked equal to the fused
-    scan's.  `rows_per_s` is n over the BinDex time.  `GB_s` credits the
-    bytes of the plan the BinDex planner picks, costed the way bindex_query
-    (csrc/bindex.cu) costs it, here from exact ranks: the result write,
-    every filter vector read, and 12 B per re-tested row (its row id, its
-    gathered value and its result word).  A query whose matches are cheaper
-    to re-test than to sieve starts from zero and re-tests those rows only
-    ("refine_only")."""
+def event_median(torch, fn, reps=9, warm=3):
+    """Median CUDA-event time (ms) of fn() on the current stream, each
+    repetition bracketed by its own events and a synchronize."""
+    st = torch.cuda.current_stream()
+    for _ in range(warm):
+        fn()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def single_leg(torch, R, D, dev, n, hbm_peak):
+    """The plain single-query scan: one uniform 2^32 column of n rows, one
+    range at 10 % selectivity ([q45, q55] of a sample), one fused-scan launch.
+    Bytes: 4 B per row read + the bitmap written (+ the 8-byte count)."""
+    col = gpu_column(torch, "uniform", n, 42, dev)
+    c = R.Context(dev.index or 0)
+    c.attach_columns([col.data_ptr()], n)
+    terms = [(0, *D.range_for_selectivity(host_sample(torch, col), 0.10))]
+    bm = torch.empty(R.bitmap_words(n), dtype=torch.int32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    ms = event_median(torch, lambda: c.scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s), reps=15)
+    nbytes = 4 * n + R.bitmap_words(n) * 4 + 8
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    out = {"workload": f"{n:.3g} rows x 1 uniform column, one 10 % range", "kernel": "scan_fused_kernel<1,1>",
+           "launches": 1, "lo": terms[0][1], "hi": terms[0][2], "selectivity": round(int(cnt.item()) / n, 5),
+           "ms": round(ms, 4), "rows_per_s": round(n / (ms * 1e-3), 1), "bytes": nbytes,
+           "GB_s": round(gbs, 1), "frac": round(gbs / hbm_peak, 4), "peak": hbm_peak}
+    c.close()
+    return out
+
+
+def multi_leg(torch, R, D, dev, n, hbm_peak, seed=3):
+    """Conjunctions over the first 2, 3 and 4 of four independently seeded
+    uniform 2^32 columns, per-column selectivity uniform in [5 %, 50 %]:
+    the fused scan (one launch: every column read once, one bitmap write)
+    against separate per-column passes plus AND passes, bitmaps compared.
+    Bytes: fused 4cN + N/8; separate c(4N + N/8) + (c-1) 3N/8."""
+    cols = [gpu_column(torch, "uniform", n, 61 + i, dev) for i in range(4)]
+    smp = [host_sample(torch, x, seed=3 + i) for i, x in enumerate(cols)]
+    c = R.Context(dev.index or 0)
+    c.attach_columns([x.data_ptr() for x in cols], n)
+    rng = np.random.default_rng(seed)
+    words = R.bitmap_words(n)
+    a = torch.empty(words, dtype=torch.int32, device=dev)
+    b = torch.empty(words, dtype=torch.int32, device=dev)
+    ca = torch.zeros(1, dtype=torch.int64, device=dev)
+    cb = torch.zeros(1, dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    res = []
+    for k in (2, 3, 4):
+        terms = []
+        for col in range(k):
+            sel = rng.uniform(0.05, 0.5)
+            terms.append((col, *D.range_for_selectivity(smp[col], sel, rng.uniform(sel / 2, 1 - sel / 2))))
+        tf = event_median(torch, lambda: c.scan_async(terms, a.data_ptr(), ca.data_ptr(), s))
+        ts = event_median(torch, lambda: c.scan_separate_async(terms, b.data_ptr(), cb.data_ptr(), s))
+        fb = 4 * k * n + words * 4
+        sb = k * (4 * n + words * 4) + (k - 1) * 3 * words * 4
+        res.append({"columns": k, "selectivity": round(int(ca.item()) / n, 6),
+                    "fused_ms": round(tf, 4), "fused_GB_s": round(fb / (tf * 1e-3) / 1e9, 1),
+                    "fused_frac": round(fb / (tf * 1e-3) / 1e9 / hbm_peak, 4),
+                    "separate_ms": round(ts, 4), "separate_GB_s": round(sb / (ts * 1e-3) / 1e9, 1),
+                    "fused_speedup_vs_separate": round(ts / tf, 3),
+                    "equal": bool(torch.equal(a, b)) and int(ca.item()) == int(cb.item())})
+    c.close()
+    return {"workload": f"{n:.3g} rows x 2-4 uniform columns, one conjunctive query", "queries": res}
+
+
+SWEEP_SELS = (0.001, 0.01, 0.10, 0.50, 0.90)
+
+
+def domain_range(domain, sel):
+    """The central run of values of a uniform [0, domain) column whose share
+    is nearest to `sel` (at least one value)."""
+    w = max(1, min(domain, int(round(sel * domain))))
+    lo = (domain - w) // 2
+    return lo, lo + w - 1
+
+
+def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
+    """One-column queries of the selectivity sweep, each through the fused
+    scan and through the BinDex (built once per column, K areas), bitmaps
+    compared: a uniform 2^32 column at 0.1/1/10/50/90 % (bounds at sample
+    quantiles) and columns of 256 and 64 distinct values (central value runs
+    nearest those shares; the achieved selectivity is reported).  Fused
+    bytes: 4N + N/8.  BinDex bytes are those of the plan its planner picks,
+    from exact ranks, costed as bindex_query (csrc/bindex.cu) costs it: the
+    result write, every filter vector read, and 12 B per re-tested row (its
+    row id, its gathered value and its result word); a query whose matches
+    are cheaper to re-test than to sieve starts from zero and re-tests those
+    rows only (refine_only)."""
     s = torch.cuda.current_stream()
-    bm = torch.empty((n + 31) // 32, dtype=torch.int32, device=dev)
+    words = R.bitmap_words(n)
+    bm = torch.empty(words, dtype=torch.int32, device=dev)
     ref = torch.empty_like(bm)
     cnt = torch.zeros(1, dtype=torch.int64, device=dev)
     res = {"rows": n, "K": K, "queries": []}
-
-    def timed(fn, reps=7):
-        for _ in range(3):
-            fn()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(s)
-            fn()
-            e1.record(s)
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return sorted(ts)[reps // 2]
-
-    for kind, seed in (("uniform", 31), ("range:0:256", 41)):
+    fused_bytes = 4 * n + words * 4
+    for kind, seed in (("uniform", 31), ("range:0:256", 41), ("range:0:64", 51)):
         col = gpu_column(torch, kind, n, seed, dev)
         c = R.Context(dev.index or 0)
         c.attach_columns([col.data_ptr()], n)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         c.build_bindex(0, K)
+        torch.cuda.synchronize()
+        build_ms = (time.perf_counter() - t0) * 1e3
         srt = torch.sort(col.to(torch.int64) & 0xFFFFFFFF).values
-        lower = lambda b: int(torch.searchsorted(srt, torch.tensor([b], device=dev)).item())
+        lower = lambda v: int(torch.searchsorted(srt, torch.tensor([v], device=dev)).item())
         fr = [lower(int(srt[k * (n // K)].item())) for k in range(K)]  # rank of area k's start value
 
         def nearest(est):  # the planner's filter vector (or constant) nearest to rank est
@@ -625,10 +797,12 @@ def bindex_query_leg(torch, R, D, dev, n, K=128):
 
         if kind == "uniform":
             smp = host_sample(torch, col)
-            qs = [D.range_for_selectivity(smp, sel) for sel in (0.001, 0.01, 0.10, 0.50, 0.90)]
+            qs = [(sel, *D.range_for_selectivity(smp, sel)) for sel in SWEEP_SELS]
         else:
-            qs = [(3, 3), (0, 25), (64, 191), (10, 250)]
-        for lo, hi in qs:
+            dom = int(kind.split(":")[2])
+            qs = [(sel, *domain_range(dom, sel)) for sel in SWEEP_SELS]
+            qs = [q for i, q in enumerate(qs) if i == 0 or q[1:] != qs[i - 1][1:]]
+        for sel, lo, hi in qs:
             terms = [(0, lo, hi)]
             r_lo = lower(lo) if lo > 0 else 0
             r_hi = lower(hi + 1) if hi < 0xFFFFFFFF else n
@@ -643,15 +817,22 @@ def bindex_query_leg(torch, R, D, dev, n, K=128):
             cand_cost = n / 8 + (match + 2048) * 40.0
             refine_only = cand_cost < sieve_cost
             nbytes = n / 8 + match * 12 if refine_only else n / 8 * (1 + fv_reads) + refine * 12
-            t_b = timed(lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream))
+            t_b = event_median(torch, lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream),
+                               reps=7)
             hits = int(cnt.item())
-            t_f = timed(lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream))
+            t_f = event_median(torch, lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream),
+                               reps=7)
+            fgbs = fused_bytes / (t_f * 1e-3) / 1e9
             res["queries"].append({
-                "column": kind, "lo": lo, "hi": hi, "selectivity": round(hits / n, 5),
-                "bindex_us": round(t_b * 1e3, 1), "fused_us": round(t_f * 1e3, 1),
-                "rows_per_s": round(n / (t_b * 1e-3), 1), "plan": "refine_only" if refine_only else "sieve",
-                "refined_rows": match if refine_only else refine, "bytes_MB": round(nbytes / 1e6, 2),
-                "GB_s": round(nbytes / (t_b * 1e-3) / 1e9, 1), "equal": bool(torch.equal(bm, ref))})
+                "column": kind, "target": sel, "lo": lo, "hi": hi, "selectivity": round(hits / n, 5),
+                "fused_us": round(t_f * 1e3, 1), "fused_GB_s": round(fgbs, 1), "fused_frac": round(fgbs / hbm_peak, 4),
+                "bindex_us": round(t_b * 1e3, 1), "bindex_rows_per_s": round(n / (t_b * 1e-3), 1),
+                "bindex_plan": "refine_only" if refine_only else "sieve",
+                "bindex_refined_rows": match if refine_only else refine, "bindex_bytes_MB": round(nbytes / 1e6, 2),
+                "bindex_GB_s": round(nbytes / (t_b * 1e-3) / 1e9, 1),
+                "bindex_frac": round(nbytes / (t_b * 1e-3) / 1e9 / hbm_peak, 4),
+                "equal": bool(torch.equal(bm, ref)) and hits == int(cnt.item())})
+        res.setdefault("bindex_build_ms", {})[kind] = round(build_ms, 1)
         c.close()
         del col, srt
         torch.cuda.empty_cache()
@@ -783,6 +964,15 @@ def served_leg(torch, R, D, ctx, dev, rank, args):
                                  "p50_ms": round(float(np.percentile(ok, 50)), 3),
                                  "p99_ms": round(float(np.percentile(ok, 99)), 3),
                                  "p999_ms": round(float(np.percentile(ok, 99.9)), 3)})
+        # the highest offered rate the server kept up with: every request
+        # admitted (none rejected) and completions within 2 % of the offer
+        kept = [r for r in out["rates"] if r["rejected"] == 0 and r["achieved_qps"] >= 0.98 * r["offered_qps"]]
+        if kept:
+            top = max(kept, key=lambda r: r["offered_qps"])
+            out["max_sustained"] = {k: top[k] for k in ("offered_qps", "achieved_qps", "p50_ms", "p99_ms", "p999_ms")}
+        over = [r for r in out["rates"] if r not in kept]
+        if over:
+            out["first_overloaded"] = min(over, key=lambda r: r["offered_qps"])["offered_qps"]
         q4 = R.prepare(D.batch_queries(samples, 256, seed=4, min_cols=4, max_cols=4))
         t0 = time.perf_counter()
         lat = srv.replay(q4, np.zeros(256))
@@ -806,8 +996,39 @@ def workload_config(wl, n, nq, kinds):
             "column_kinds": kinds, "l2": f"inputs larger than L2 ({n * 4 / 1e6:.0f} MB per column)"}
 
 
+def reference_columns(kinds, n):
+    """The workload's columns on the host: generated exactly as the GPU arm
+    generates them (same device generator and seeds, rank 0), so both arms
+    answer the same queries on the same rows; the numpy generators of the
+    same distributions stand in where no GPU is visible."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            dev = torch.device("cuda", 0)
+            out = []
+            for i, k in enumerate(kinds):
+                col = gpu_column(torch, k, n, 1000 + i, dev)
+                smp = host_sample(torch, col, seed=7 + i)
+                out.append((col.cpu().numpy().view(np.uint32).copy(), smp))
+                del col
+            torch.cuda.empty_cache()
+            return [c for c, _ in out], [m for _, m in out], "device generator of the GPU arm (same rows)"
+    except Exception:  # fall back to the host generators below
+        pass
+    cols = cpu_sample_columns(kinds, n)
+    smp = [np.sort(c[np.random.default_rng(7).integers(0, n, size=1 << 18)]) for c in cols]
+    return cols, smp, "numpy generators of the same distributions"
+
+
 def run_reference(args):
-    """--impl reference: the reference's CPU path on this host, rank 0 only."""
+    """--impl reference: the reference's own CPU path (its bindex.cpp
+    compiled unmodified, oracle/_ref) on this host, rank 0 only, on the
+    workload's own row count: the BinDex of every column is built once
+    (reported, not timed), then every step times `per_step` of the
+    workload's queries through the reference's query loop (sieve + refine
+    + AND merge per query, its timer-11 region), a disjoint seeded subset
+    per step.  Without a harness binary for the workload's row count the
+    2^24-row binary runs a prefix sample, and the line says so."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
@@ -818,42 +1039,64 @@ def run_reference(args):
                           "the bitmap); the q6 line's cpu_baseline times a numpy port"}), flush=True)
         return
     kinds = {"single": ["uniform"], "multi": ["uniform"] * 4}.get(wl, BATCH_KINDS)
-    cols = cpu_sample_columns(kinds, REF_N)
-    smp = [np.sort(c[np.random.default_rng(7).integers(0, REF_N, size=1 << 18)]) for c in cols]
-    queries = make_queries(D, wl, smp, args.queries)
-    bprq = row_query_bytes(REF_N, queries)
-    per_step = min(len(queries), 8)
-    vals, kind, cores, detail = [], None, None, {}
+    n_full = args.nrows
+    n = n_full if reference_binary(n_full) else REF_N
+    binary = reference_binary(n)
     t_start = time.time()
-    for step in range(args.warmup + args.steps):
-        qs = [queries[(step * per_step + i) % len(queries)] for i in range(per_step)]
-        sec, kind, cores, detail = cpu_reference_run(cols, qs, repeats=1)
-        if step >= args.warmup:
-            vals.append((REF_N * bprq / sec / 1e9, 1.0 / sec))
-        if step >= args.warmup and time.time() - t_start > 150:
-            break
-    v = statistics.median(x[0] for x in vals)
-    qps = statistics.median(x[1] for x in vals)
+    cols, smp, source = reference_columns(kinds, n_full if n == n_full else n)
+    queries = make_queries(D, wl, smp, args.queries)
+    bprq = row_query_bytes(n_full, queries)
+    nq = len(queries)
+    per_step = min(nq, args.ref_queries_per_step)
+    order = np.random.default_rng(2024).permutation(nq)
+    steps = args.warmup + args.steps
+    picks = [[int(order[(st * per_step + i) % nq]) for i in range(per_step)] for st in range(steps)]
+    if binary:
+        flat = [queries[i] for p in picks for i in p]
+        build_ms, ms, eq = run_reference_harness(binary, cols, flat, checked=1)
+        kind, cores = "reference", REF_THREADS
+        detail = {"reference_bindex_equals_scalar_checked": all(eq), "checked_queries": len(eq),
+                  "index_build_ms": round(build_ms)}
+    else:  # the oracle's restatement, one thread
+        from oracle import oracle as O
+        ms = []
+        for p in picks:
+            for i in p:
+                q = queries[i]
+                t0 = time.perf_counter()
+                O.range_scan([cols[c] for c, _, _ in q], [t[1] for t in q], [t[2] for t in q])
+                ms.append((time.perf_counter() - t0) * 1e3)
+        kind, cores, detail = "port", 1, {}
+    del cols
+    step_ms = [sum(ms[st * per_step:(st + 1) * per_step]) for st in range(steps)][args.warmup:]
+    vals = [per_step * n * bprq / (t * 1e-3) / 1e9 for t in step_ms]
+    v = statistics.median(vals)
+    t_med = statistics.median(step_ms)
+    qps = per_step / (t_med * 1e-3) * n / n_full
+    sample = (f"{n} rows x {len(kinds)} columns ({source}); each step {per_step} of the workload's {nq} queries "
+              f"(seeded disjoint subsets, {len(picks) * per_step} queries over {steps} steps) through the "
+              f"reference BinDex query loop, {cores} threads, index build excluded; credited {bprq:.4f} B per row "
+              "and query, the workload's bytes share")
+    if n != n_full:
+        sample += f"; a prefix sample of the workload's {n_full} rows, queries_per_s scaled to them"
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "n_gpus": world,
-            "steps": len(vals), "warmup": args.warmup, "ms_per_step": round(1e3 * per_step / qps, 3),
+            "steps": len(step_ms), "warmup": args.warmup, "ms_per_step": round(t_med, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded)",
-            "config": workload_config(wl, args.nrows, len(queries), kinds),
-            "queries_per_s": round(qps * REF_N / args.nrows, 3),
-            "queries_per_s_sample": round(qps, 2),
+            "config": workload_config(wl, n_full, nq, kinds),
+            "rows_run": n, "queries_timed_per_step": per_step,
+            "queries_per_s": round(qps, 3),
             "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "kind": kind, "cores": cores,
-                             "sample": f"{REF_N} rows x {len(cols)} columns, {per_step} of the workload's "
-                                       f"{len(queries)} queries per step (reference BinDex query loop, index "
-                                       f"build excluded); credited {bprq:.4f} B per row and query, the "
-                                       "workload's bytes share; queries_per_s scaled to the workload's rows",
-                             **detail},
+                             "sample": sample, **host_info(), **detail,
+                             "wall_s": round(time.time() - t_start, 1)},
             "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--gpus", type=int, default=1, help="ranks, one per GPU (started under torchrun if needed)")
+    ap.add_argument("--dry-run", action="store_true", help="print each rank's world and exit (no GPU work)")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -861,21 +1104,33 @@ def main():
     ap.add_argument("--nrows", type=int, default=100_000_000)
     ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-queries-per-step", type=int, default=32,
+                    help="--impl reference: queries of the workload timed per step")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-compare", action="store_true", help="skip the one-query-per-launch comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-scan leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default batch launch shape")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the single-column, multi-column and selectivity-sweep legs (profiling runs)")
     ap.add_argument("--bindex-io", type=int, default=0, metavar="ROWS",
                     help="also time BinDex build vs save and load for a ROWS-row column (off by default)")
     ap.add_argument("--bindex-query", type=int, default=0, metavar="ROWS",
-                    help="also time single-column BinDex queries against fused scans on ROWS-row columns")
+                    help="run the selectivity sweep (fused scan and BinDex) on ROWS-row columns alone")
     ap.add_argument("--pass-sweep", type=int, default=0, metavar="ROWS",
                     help="also time one pass of 1..512 queries over a ROWS-row table (off by default)")
     ap.add_argument("--serve-rows", type=int, default=1 << 28)
-    ap.add_argument("--serve-rates", type=float, nargs="+", default=[1000, 5000, 10000])
+    ap.add_argument("--serve-rates", type=float, nargs="+",
+                    default=[1000, 5000, 10000, 20000, 30000, 40000, 50000])
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    cmd = check_world(args.gpus)
+    if cmd is not None:  # start the ranks and report their exit status
+        raise SystemExit(subprocess.run(cmd).returncode)
+    if args.dry_run:  # the resolved world, without touching a GPU
+        world, rank, local = dist_env()
+        print(json.dumps({"rank": rank, "local_rank": local, "world": world, "gpus": args.gpus}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
