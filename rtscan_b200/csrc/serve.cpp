@@ -18,7 +18,14 @@
 //   * The worker thread plans the active set (mask tables) only when it
 //     changes, keeps at most `max_inflight_steps` steps queued on its stream,
 //     and marks a request done when the event recorded after its last step
-//     has completed.
+//     has completed.  Planning and the plan upload (which waits for the
+//     steps still reading the other plan buffer) run without the server
+//     lock, so submitters and pollers never wait behind them; the lock
+//     covers admission, the step's launches and the bookkeeping only.
+//   * A finished request's count is copied to pinned host memory on the
+//     scan stream right after its last step (one 8-byte copy each), so
+//     poll/wait/fetch read it without touching the device; a bitmap fetch
+//     copies outside the lock.
 // Requests the batched kernel does not take (an empty term, no constrained
 // column, more than eight columns) are answered in one launch at admission.
 #include <cuda_runtime.h>
@@ -44,7 +51,10 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-enum SlotState { FREE = 0, ACTIVE, FINISHING, DONE, CANCELLING };
+// FREE -> ACTIVE (scanning) -> FINISHING (last step queued) -> DONE ->
+// FETCHING (a bitmap copy in progress) -> FREE; ACTIVE/FINISHING ->
+// CANCELLING -> FREE once the steps queued before the cancel are done.
+enum SlotState { FREE = 0, ACTIVE, FINISHING, DONE, CANCELLING, FETCHING };
 
 struct Request {
   uint64_t ticket;
@@ -61,6 +71,7 @@ struct rts_server {
   int nseg = 0;
   uint32_t *bitmaps = nullptr;
   unsigned long long *counts = nullptr;
+  unsigned long long *host_counts = nullptr;  // pinned; slot i's count once it is DONE
   cudaStream_t stream = nullptr, copy_stream = nullptr;
 
   struct PlanBuf {
@@ -120,6 +131,8 @@ struct rts_server {
   }
   void put_event(cudaEvent_t e) { event_pool.push_back(e); }
 
+  // Copy a plan blob into the plan buffer not used by the previous plan,
+  // after the steps that still read it (worker thread, lock not held).
   void upload(const std::vector<uint32_t> &blob) {
     PlanBuf &b = pb[next_pb];
     next_pb ^= 1;
@@ -170,9 +183,7 @@ struct rts_server {
         std::vector<rts::NormQuery> one(slots.size());
         one[sl] = S.q;
         ctx->launches += rts::launch_outside(ctx, one, {sl}, nullptr, bitmaps, stride, counts, stream);
-        S.ev = get_event();
-        RTS_CUDA(cudaEventRecord(S.ev, stream));
-        S.state = FINISHING;
+        finish(sl);
       } else {
         RTS_CUDA(cudaMemsetAsync(counts + sl, 0, 8, stream));
         S.state = ACTIVE;
@@ -181,19 +192,48 @@ struct rts_server {
     }
   }
 
-  void step() {
-    rts::Range nvtx_range_("rts_server_step");
-    std::vector<int> active;
+  // Queue the copy of slot sl's count to the host and the event that marks
+  // the slot done, behind every launch that writes it (mu held).
+  void finish(int sl) {
+    Slot &S = slots[sl];
+    RTS_CUDA(cudaMemcpyAsync(host_counts + sl, counts + sl, 8, cudaMemcpyDeviceToHost, stream));
+    S.ev = get_event();
+    RTS_CUDA(cudaEventRecord(S.ev, stream));
+    S.state = FINISHING;
+  }
+
+  // Slots cancelled while active get their release event here, after every
+  // launch queued so far, some of which may still write them (mu held).
+  void fence_cancels() {
+    for (auto &S : slots)
+      if (S.state == CANCELLING && !S.ev) {
+        S.ev = get_event();
+        RTS_CUDA(cudaEventRecord(S.ev, stream));
+      }
+  }
+
+  // The active set, and a copy of its queries when it differs from the
+  // planned one (mu held): -1 nothing is active, 0 the plan is current, 1
+  // `norm` holds the queries to plan.  Only the worker admits and retires
+  // requests, so until the step is launched the set can lose cancelled
+  // slots only.
+  int snapshot(std::vector<int> &active, std::vector<rts::NormQuery> &norm, uint64_t &version) {
+    active.clear();
     for (size_t i = 0; i < slots.size(); i++)
       if (slots[i].state == ACTIVE) active.push_back((int)i);
-    if (active.empty()) return;
-    if (plan_version != active_version) {
-      std::vector<rts::NormQuery> norm(slots.size());
-      for (int sl : active) norm[sl] = slots[sl].q;
-      plan = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget);
-      upload(rts::batch_plan_blob(*plan));
-      plan_version = active_version;
-    }
+    if (active.empty()) return -1;
+    if (plan_version == active_version) return 0;
+    norm.assign(slots.size(), rts::NormQuery());
+    for (int sl : active) norm[sl] = slots[sl].q;
+    version = active_version;
+    return 1;
+  }
+
+  // Launch one step of the current plan over the segment at the cursor and
+  // retire the requests that have now seen every segment (mu held).
+  void step() {
+    rts::Range nvtx_range_("rts_server_step");
+    if (!plan || plan_slots.empty()) return;
     const uint64_t r0 = (uint64_t)cursor * seg_rows;
     const uint64_t r1 = std::min<uint64_t>(nrows, r0 + seg_rows);
     ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, stream);
@@ -205,12 +245,11 @@ struct rts_server {
     steps++;
     cursor = (cursor + 1) % nseg;
     bool changed = false;
-    for (int sl : active) {
+    for (int sl : plan_slots) {
       Slot &S = slots[sl];
+      if (S.state != ACTIVE) continue;  // cancelled since the plan was made
       if (++S.segs_done == nseg) {
-        S.ev = get_event();
-        RTS_CUDA(cudaEventRecord(S.ev, stream));
-        S.state = FINISHING;
+        finish(sl);
         changed = true;
       }
     }
@@ -223,6 +262,7 @@ struct rts_server {
     for (size_t i = 0; i < slots.size(); i++) {
       Slot &S = slots[i];
       if (S.state != FINISHING && S.state != CANCELLING) continue;
+      if (!S.ev) continue;  // a cancel not fenced yet
       cudaError_t e = cudaEventQuery(S.ev);
       if (e == cudaErrorNotReady) continue;
       if (e != cudaSuccess) throw rts::Error(RTS_ERR_CUDA, std::string("server step: ") + cudaGetErrorString(e));
@@ -246,6 +286,8 @@ struct rts_server {
   void run() {
     cudaSetDevice(ctx->device);
     try {
+      std::vector<int> active;
+      std::vector<rts::NormQuery> norm;
       while (!stop.load()) {
         // bound the steps queued on the stream, without holding the lock
         std::vector<cudaEvent_t> retired;
@@ -254,10 +296,13 @@ struct rts_server {
           retired.push_back(inflight.front());
           inflight.pop_front();
         }
+        uint64_t version = 0;
+        int todo = -1;
         {
           std::unique_lock<std::mutex> lk(mu);
           for (auto e : retired) put_event(e);
           admit();
+          fence_cancels();
           reap();
           bool busy = false;
           for (auto &S : slots)
@@ -266,7 +311,24 @@ struct rts_server {
             cv_work.wait_for(lk, std::chrono::milliseconds(2));
             continue;
           }
+          todo = snapshot(active, norm, version);
+          if (todo < 0) {  // only finishing or cancelled requests: wait for their events
+            fence_cancels();
+            cv_work.wait_for(lk, std::chrono::microseconds(200));
+            continue;
+          }
+        }
+        if (todo == 1) {  // plan and upload without the lock
+          rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget);
+          upload(rts::batch_plan_blob(*p));
+          plan = std::move(p);
+          plan_slots = active;
+          plan_version = version;
+        }
+        {
+          std::lock_guard<std::mutex> lk(mu);
           step();
+          fence_cancels();
         }
         // let clients in between steps
         std::this_thread::yield();
@@ -299,6 +361,7 @@ struct rts_server {
       if (S.ev) cudaEventDestroy(S.ev);
     if (bitmaps) cudaFree(bitmaps);
     if (counts) cudaFree(counts);
+    if (host_counts) cudaFreeHost(host_counts);
     if (stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
@@ -371,6 +434,7 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
       cudaGetLastError();
       throw rts::Error(RTS_ERR_NOMEM, "result pool of " + std::to_string(bm_bytes) + " bytes does not fit");
     }
+    RTS_CUDA(cudaMallocHost(&srv->host_counts, (size_t)c.max_active * 8));
     RTS_CUDA(cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking));
     RTS_CUDA(cudaStreamCreateWithFlags(&srv->copy_stream, cudaStreamNonBlocking));
     srv->slots.resize(c.max_active);
@@ -423,14 +487,9 @@ rts_status rts_server_poll(rts_server *srv, uint64_t ticket, int32_t *done, uint
       return fail(srv, RTS_ERR_ARG, "unknown ticket");
     }
     rts_server::Slot &S = srv->slots[it->second];
-    if (S.state == DONE) {
+    if (S.state == DONE || S.state == FETCHING) {
       *done = 1;
-      if (count) {
-        unsigned long long c = 0;
-        cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
-        cudaStreamSynchronize(srv->copy_stream);
-        *count = c;
-      }
+      if (count) *count = srv->host_counts[it->second];
     }
     return RTS_OK;
   });
@@ -444,13 +503,9 @@ rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms,
     while (true) {
       if (!srv->fatal.empty()) return fail(srv, RTS_ERR_CUDA, "server stopped: " + srv->fatal);
       auto it = srv->ticket_slot.find(ticket);
-      if (it != srv->ticket_slot.end() && srv->slots[it->second].state == DONE) {
-        if (count) {
-          unsigned long long c = 0;
-          cudaMemcpyAsync(&c, srv->counts + it->second, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
-          cudaStreamSynchronize(srv->copy_stream);
-          *count = c;
-        }
+      if (it != srv->ticket_slot.end() &&
+          (srv->slots[it->second].state == DONE || srv->slots[it->second].state == FETCHING)) {
+        if (count) *count = srv->host_counts[it->second];
         return RTS_OK;
       }
       if (it == srv->ticket_slot.end()) {
@@ -460,7 +515,9 @@ rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms,
       }
       if (srv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
         auto it2 = srv->ticket_slot.find(ticket);
-        if (it2 != srv->ticket_slot.end() && srv->slots[it2->second].state == DONE) continue;
+        if (it2 != srv->ticket_slot.end() &&
+            (srv->slots[it2->second].state == DONE || srv->slots[it2->second].state == FETCHING))
+          continue;
         return fail(srv, RTS_ERR_TIMEOUT, "request not done within the timeout");
       }
     }
@@ -470,23 +527,38 @@ rts_status rts_server_wait(rts_server *srv, uint64_t ticket, int32_t timeout_ms,
 rts_status rts_server_fetch(rts_server *srv, uint64_t ticket, uint32_t *host_bitmap, uint64_t *count) {
   return srv_guarded(srv, [&]() -> rts_status {
     if (!srv) return fail(srv, RTS_ERR_ARG, "null server");
-    std::lock_guard<std::mutex> lk(srv->mu);
-    auto it = srv->ticket_slot.find(ticket);
-    if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown or unfinished ticket");
-    const int sl = it->second;
-    rts_server::Slot &S = srv->slots[sl];
-    if (S.state != DONE) return fail(srv, RTS_ERR_STATE, "request not done");
-    cudaError_t e = cudaSuccess;
-    if (host_bitmap)
-      e = cudaMemcpyAsync(host_bitmap, srv->bitmaps + (uint64_t)sl * srv->stride, srv->words * 4,
-                          cudaMemcpyDeviceToHost, srv->copy_stream);
-    unsigned long long c = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&c, srv->counts + sl, 8, cudaMemcpyDeviceToHost, srv->copy_stream);
+    int sl;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      auto it = srv->ticket_slot.find(ticket);
+      if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown or unfinished ticket");
+      sl = it->second;
+      rts_server::Slot &S = srv->slots[sl];
+      if (S.state == FETCHING) return fail(srv, RTS_ERR_STATE, "request is being fetched by another call");
+      if (S.state != DONE) return fail(srv, RTS_ERR_STATE, "request not done");
+      if (count) *count = srv->host_counts[sl];
+      if (!host_bitmap) {  // the count is already on the host: release the slot
+        S.state = FREE;
+        srv->ticket_slot.erase(it);
+        srv->free_slots.push_back(sl);
+        srv->cv_work.notify_one();
+        return RTS_OK;
+      }
+      S.state = FETCHING;  // nobody frees or reuses the slot during the copy
+    }
+    // the bitmap leaves without the lock held
+    rts::DeviceGuard device_guard(srv->ctx->device);
+    cudaError_t e = cudaMemcpyAsync(host_bitmap, srv->bitmaps + (uint64_t)sl * srv->stride, srv->words * 4,
+                                    cudaMemcpyDeviceToHost, srv->copy_stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(srv->copy_stream);
-    if (e != cudaSuccess) return fail(srv, RTS_ERR_CUDA, std::string("fetch: ") + cudaGetErrorString(e));
-    if (count) *count = c;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    rts_server::Slot &S = srv->slots[sl];
+    if (e != cudaSuccess) {
+      S.state = DONE;  // the caller may try again
+      return fail(srv, RTS_ERR_CUDA, std::string("fetch: ") + cudaGetErrorString(e));
+    }
     S.state = FREE;
-    srv->ticket_slot.erase(it);
+    srv->ticket_slot.erase(ticket);
     srv->free_slots.push_back(sl);
     srv->cv_work.notify_one();
     return RTS_OK;
@@ -506,12 +578,13 @@ rts_status rts_server_cancel(rts_server *srv, uint64_t ticket) {
     auto it = srv->ticket_slot.find(ticket);
     if (it == srv->ticket_slot.end()) return fail(srv, RTS_ERR_ARG, "unknown ticket");
     rts_server::Slot &S = srv->slots[it->second];
+    if (S.state == FETCHING) return fail(srv, RTS_ERR_STATE, "request is being fetched");
     if (S.state == ACTIVE) {
-      // kernels already queued may still write this slot: free it after them
-      S.ev = srv->get_event();
-      cudaEventRecord(S.ev, srv->stream);
+      // kernels already queued (or being queued by the worker) may still
+      // write this slot: the worker records its release event after them
       S.state = CANCELLING;
       srv->active_version++;
+      srv->cv_work.notify_one();
     } else if (S.state == FINISHING) {
       S.state = CANCELLING;
     } else if (S.state == DONE) {
@@ -574,7 +647,9 @@ rts_status rts_server_stop(rts_server *srv) {
 // Open-loop replay for benchmarks: request q is submitted at arrival_s[q]
 // seconds after the call starts, and its result slot is released as soon
 // as it is done.  latency_ms[q] receives submit-to-done time (or -1 when
-// the queue was full).  Blocks until every request is done.
+// the queue was full).  Blocks until every request is done.  A replay that
+// stops on an error (a request the server refuses, a failed release)
+// cancels its requests still in flight before it returns.
 rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32_t *offsets, int32_t nq,
                              const double *arrival_s, double *latency_ms) {
   return srv_guarded(srv, [&]() -> rts_status {
@@ -650,10 +725,13 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
           auto it = index_of.find(d.first);
           if (it == index_of.end()) continue;  // not one of this replay's requests
           q = it->second;
-          index_of.erase(it);
         }
         rc = rts_server_fetch(srv, d.first, nullptr, nullptr);
-        if (rc != RTS_OK) break;
+        if (rc != RTS_OK) break;  // the ticket stays listed and is cancelled below
+        {
+          std::lock_guard<std::mutex> ml(map_mu);
+          index_of.erase(d.first);
+        }
         latency_ms[q] = (d.second - t_sub[q]) * 1e3;
         finished++;
       }
@@ -667,6 +745,13 @@ rts_status rts_server_replay(rts_server *srv, const rts_term *terms, const int32
       srv->done_tickets.clear();
     }
     if (rc == RTS_OK) rc = prod_err.load();
+    // stopped early: release this replay's requests still queued, running or
+    // done, so that their result slots return to the pool
+    if (rc != RTS_OK) {
+      std::lock_guard<std::mutex> ml(map_mu);
+      for (auto &kv : index_of) rts_server_cancel(srv, kv.first);
+      index_of.clear();
+    }
     if (rc != RTS_OK && rc != RTS_ERR_CUDA) return rc;
     if (rc == RTS_ERR_CUDA) return fail(srv, rc, "server stopped: " + srv->fatal);
     return RTS_OK;

@@ -133,3 +133,25 @@ def test_replay_open_loop(ctx, table):
         assert (lat > 0).all()
         st = srv.stats()
         assert st["completed"] == len(qs)
+
+
+def test_replay_stopped_by_a_refused_request_releases_its_slots(ctx, table):
+    """A replay that stops partway (here the server refuses a request whose
+    column does not exist) cancels its requests still in flight: no result
+    slot stays held, and the server answers later requests in full."""
+    ctx.load_columns(table)
+    good = D.batch_queries(table, 40, seed=11)
+    qs = good[:25] + [[(99, 0, 10)]] + good[25:]
+    arrivals = np.linspace(0, 0.01, len(qs))
+    with R.Server(ctx, max_active=8, segment_rows=1 << 18) as srv:
+        with pytest.raises(R.RtsError) as e:
+            srv.replay(qs, arrivals)
+        assert e.value.code == -1  # RTS_ERR_ARG, the refused submit
+        assert srv.stats()["active"] == 0
+        # every slot is free again: max_active requests run at once
+        tks = [srv.submit(q) for q in good[:8]]
+        for q, tk in zip(good[:8], tks):
+            srv.wait(tk, 60000)
+            assert srv.fetch(tk, want_bitmap=False)[1] == alone(ctx, q)[1]
+        lat = srv.replay(good, np.linspace(0, 0.01, len(good)))
+        assert (lat > 0).all()
