@@ -98,15 +98,20 @@ __global__ void sample_kernel(const uint32_t *sval, uint64_t n, uint32_t *out, u
 // fv[k] word w: bit 31-r set iff row 32w+r < n and col[32w+r] < S[k+1].
 // A thread owns one word; a(x) = #{i in 1..K-1 : S[i] <= x} is found by a
 // binary search over the start values in shared memory, and fv[k] holds the
-// rows with a(x) <= k.
+// rows with a(x) <= k.  A (uint8_t for K <= 256, else uint16_t) holds a(x);
+// its largest value marks the padding rows past n, which no fv[k] holds.
+// With kCheck the words are compared with fv instead of written and the
+// mismatching words counted into *bad (an index loaded from a file).
+template <typename A, bool kCheck>
 __global__ void __launch_bounds__(kThreads) fv_kernel(const uint32_t *col, uint64_t n, const uint32_t *start, int K,
-                                                      uint32_t *fv, uint64_t fv_stride) {
+                                                      uint32_t *fv, uint64_t fv_stride, unsigned long long *bad) {
   extern __shared__ uint32_t s_start[];
   for (int i = threadIdx.x; i < K; i += blockDim.x) s_start[i] = start[i];
   __syncthreads();
   const uint64_t words = (n + 31) >> 5;
+  unsigned long long b = 0;
   for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (uint64_t)gridDim.x * blockDim.x) {
-    uint8_t a[32];
+    A a[32];
     const uint64_t row0 = w * 32;
 #pragma unroll
     for (int r = 0; r < 32; r++) {
@@ -118,51 +123,38 @@ __global__ void __launch_bounds__(kThreads) fv_kernel(const uint32_t *col, uint6
           const int mid = (lo + hi) >> 1;
           if (s_start[mid] <= x) lo = mid + 1; else hi = mid;
         }
-        a[r] = (uint8_t)min(lo - 1, 255);
+        a[r] = (A)(lo - 1);
       } else {
-        a[r] = 255;  // never below any k: padding rows stay zero
+        a[r] = (A)~A(0);
       }
     }
-    // a(x) can exceed 254 only when K > 256; handled by the clamp path below.
     for (int k = 0; k < K - 1; k++) {
       uint32_t word = 0;
 #pragma unroll
       for (int r = 0; r < 32; r++) word |= (a[r] <= k ? 1u : 0u) << (31 - r);
-      fv[(uint64_t)k * fv_stride + w] = word;
+      if (kCheck) b += fv[(uint64_t)k * fv_stride + w] != word;
+      else fv[(uint64_t)k * fv_stride + w] = word;
     }
+  }
+  if (kCheck) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(kFull, b, o);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(bad, b);
   }
 }
 
-// Variant for K > 256: a(x) kept in 16 bits.
-__global__ void __launch_bounds__(kThreads) fv_kernel_wide(const uint32_t *col, uint64_t n, const uint32_t *start,
-                                                           int K, uint32_t *fv, uint64_t fv_stride) {
-  extern __shared__ uint32_t s_start[];
-  for (int i = threadIdx.x; i < K; i += blockDim.x) s_start[i] = start[i];
-  __syncthreads();
+int blocks_for(uint64_t items, int sm_count, int per_sm);
+
+template <bool kCheck>
+void launch_fv(const uint32_t *col, uint64_t n, const uint32_t *start, int K, uint32_t *fv, uint64_t fv_stride,
+               unsigned long long *bad, int sm_count, cudaStream_t s) {
   const uint64_t words = (n + 31) >> 5;
-  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (uint64_t)gridDim.x * blockDim.x) {
-    uint16_t a[32];
-    const uint64_t row0 = w * 32;
-    for (int r = 0; r < 32; r++) {
-      const uint64_t row = row0 + r;
-      if (row < n) {
-        const uint32_t x = col[row];
-        int lo = 1, hi = K;
-        while (lo < hi) {
-          const int mid = (lo + hi) >> 1;
-          if (s_start[mid] <= x) lo = mid + 1; else hi = mid;
-        }
-        a[r] = (uint16_t)(lo - 1);
-      } else {
-        a[r] = 0xFFFF;
-      }
-    }
-    for (int k = 0; k < K - 1; k++) {
-      uint32_t word = 0;
-      for (int r = 0; r < 32; r++) word |= (a[r] <= k ? 1u : 0u) << (31 - r);
-      fv[(uint64_t)k * fv_stride + w] = word;
-    }
-  }
+  if (K <= 256)
+    fv_kernel<uint8_t, kCheck><<<blocks_for(words, sm_count, 8), kThreads, K * sizeof(uint32_t), s>>>(
+        col, n, start, K, fv, fv_stride, bad);
+  else
+    fv_kernel<uint16_t, kCheck><<<blocks_for(words, sm_count, 8), kThreads, K * sizeof(uint32_t), s>>>(
+        col, n, start, K, fv, fv_stride, bad);
 }
 
 // ---- query -------------------------------------------------------------------
@@ -352,6 +344,17 @@ struct DevFree {
 };
 }  // namespace
 
+uint64_t count_fv_mismatches(const uint32_t *col, uint64_t n, const uint32_t *d_start, int K, const uint32_t *fv,
+                             uint64_t fv_stride, unsigned long long *d_bad, int sm_count, cudaStream_t s) {
+  RTS_CUDA(cudaMemsetAsync(d_bad, 0, 8, s));
+  if (K > 1) launch_fv<true>(col, n, d_start, K, const_cast<uint32_t *>(fv), fv_stride, d_bad, sm_count, s);
+  RTS_CUDA(cudaGetLastError());
+  unsigned long long bad = 0;
+  RTS_CUDA(cudaMemcpyAsync(&bad, d_bad, 8, cudaMemcpyDeviceToHost, s));
+  RTS_CUDA(cudaStreamSynchronize(s));
+  return bad;
+}
+
 std::unique_ptr<GpuBinDex> build_bindex(const uint32_t *col, uint64_t n, int K, int sm_count, cudaStream_t s) {
   if (K < 2 || K > 4096) throw Error(RTS_ERR_ARG, "K must be in [2, 4096]");
   if (n < (uint64_t)K) throw Error(RTS_ERR_ARG, "BinDex needs at least K rows");
@@ -384,13 +387,7 @@ std::unique_ptr<GpuBinDex> build_bindex(const uint32_t *col, uint64_t n, int K, 
   if (K > 1) {
     b->fv = dev_alloc<uint32_t>((size_t)(K - 1) * b->fv_stride);
     RTS_CUDA(cudaMemsetAsync(b->fv, 0, (size_t)(K - 1) * b->fv_stride * 4, s));
-    const uint64_t words = (n + 31) >> 5;
-    if (K <= 256)
-      fv_kernel<<<blocks_for(words, sm_count, 8), kThreads, K * sizeof(uint32_t), s>>>(col, n, d_start, K, b->fv,
-                                                                                      b->fv_stride);
-    else
-      fv_kernel_wide<<<blocks_for(words, sm_count, 8), kThreads, K * sizeof(uint32_t), s>>>(col, n, d_start, K, b->fv,
-                                                                                           b->fv_stride);
+    launch_fv<false>(col, n, d_start, K, b->fv, b->fv_stride, nullptr, sm_count, s);
   }
   RTS_CUDA(cudaGetLastError());
   b->start.resize(K);

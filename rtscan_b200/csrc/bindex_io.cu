@@ -15,9 +15,15 @@
 // Each checksum is sum_i mix(i, word_i) mod 2^64 over the array's 32-bit
 // words (order-dependent, computed on the device for the large arrays);
 // header_check is the same function over the header's preceding words.
-// Loading verifies every checksum, then checks the index against the
-// resident column on the device: col[spos[r]] == sval[r] and sval is
-// non-decreasing for every rank r.
+// Loading verifies every checksum, then checks the whole index against the
+// resident column on the device, so that a file whose checksums agree but
+// whose contents are wrong (written by a faulty build, or crafted) is
+// refused rather than answering queries wrongly or sending the refine past
+// the sorted arrays: col[spos[r]] == sval[r] and sval is non-decreasing for
+// every rank r; start[k] == sval[k * (n / K)]; first_rank[k] is the lower
+// bound of start[k] in sval; sample[j] == sval[j * 1024]; min/max are the
+// first and last sorted values; every filter-vector word equals the one
+// the start values give for the column, and the padding words are zero.
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdio.h>
@@ -81,6 +87,37 @@ __global__ void verify_kernel(const uint32_t *__restrict__ col, const uint32_t *
   for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t v = sval[r], row = spos[r];
     b += row >= n || col[row] != v || (r > 0 && sval[r - 1] > v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(bad, b);
+}
+
+// Counts entries of the area table, the planner's sample and the
+// filter-vector padding that disagree with the sorted values: start[k] must
+// be sval[k*(n/K)], first_rank[k] its lower bound (sval[r] == start[k] and
+// r == 0 or sval[r-1] < start[k]), sample[j] sval[j*stride], and every
+// padding word past `words` in a filter vector zero.
+__global__ void tables_kernel(const uint32_t *__restrict__ sval, uint64_t n, int K, const uint32_t *__restrict__ start,
+                              const uint64_t *__restrict__ first_rank, const uint32_t *__restrict__ sample, uint64_t m,
+                              uint64_t stride, const uint32_t *__restrict__ fv, uint64_t fv_stride, uint64_t words,
+                              unsigned long long *bad) {
+  const uint64_t pad = fv_stride - words;
+  const uint64_t total = (uint64_t)K + m + (uint64_t)(K - 1) * pad;
+  const uint64_t avg = n / (uint64_t)K;
+  unsigned long long b = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (i < (uint64_t)K) {
+      const uint32_t v = sval[i * avg];
+      const uint64_t r = first_rank[i];
+      b += start[i] != v || r > i * avg || sval[r] != v || (r > 0 && sval[r - 1] >= v);
+    } else if (i < (uint64_t)K + m) {
+      const uint64_t j = i - K;
+      b += sample[j] != sval[j * stride];
+    } else {
+      const uint64_t q = i - K - m;
+      b += fv[(q / pad) * fv_stride + words + q % pad] != 0;
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
@@ -289,9 +326,39 @@ rts_status rts_load_bindex(rts_ctx *ctx, int32_t column, const char *path) {
     unsigned long long bad = 0;
     RTS_CUDA(cudaMemcpy(&bad, scratch, 8, cudaMemcpyDeviceToHost));
     if (bad) throw rts::Error(RTS_ERR_PARSE, p + ": index does not match column " + std::to_string(column));
+    // the host tables and the filter vectors against the sorted values
+    uint32_t ends[2];
+    RTS_CUDA(cudaMemcpy(&ends[0], b->sval, 4, cudaMemcpyDeviceToHost));
+    RTS_CUDA(cudaMemcpy(&ends[1], b->sval + h.n - 1, 4, cudaMemcpyDeviceToHost));
+    if (ends[0] != h.min_val || ends[1] != h.max_val)
+      throw rts::Error(RTS_ERR_PARSE, p + ": min/max do not match the sorted values");
+    uint32_t *tables = nullptr;
+    alloc(tables, (uint64_t)h.K * 3 + 1 + h.nsample);  // start, pad word, first_rank, sample
+    struct Free {
+      void *q;
+      ~Free() { cudaFree(q); }
+    } free_tables{tables};
+    uint32_t *d_start = tables;
+    uint64_t *d_rank = reinterpret_cast<uint64_t *>(tables + ((h.K + 1) & ~1u));
+    uint32_t *d_sample = reinterpret_cast<uint32_t *>(d_rank + h.K);
+    RTS_CUDA(cudaMemcpy(d_start, b->start.data(), h.K * 4, cudaMemcpyHostToDevice));
+    RTS_CUDA(cudaMemcpy(d_rank, ranks.data(), h.K * 8, cudaMemcpyHostToDevice));
+    RTS_CUDA(cudaMemcpy(d_sample, b->sample.data(), h.nsample * 4, cudaMemcpyHostToDevice));
+    RTS_CUDA(cudaMemset(scratch, 0, 8));
+    const uint64_t words = (h.n + 31) >> 5;
+    const uint64_t items = h.K + h.nsample + (uint64_t)(h.K - 1) * (h.fv_stride - words);
+    const int tgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((items + 255) / 256, (uint64_t)ctx->sm_count * 8));
+    rts::tables_kernel<<<tgrid, 256>>>(b->sval, h.n, (int)h.K, d_start, d_rank, d_sample, h.nsample,
+                                       rts::kSampleStride, b->fv, h.fv_stride, words, scratch);
+    RTS_CUDA(cudaGetLastError());
+    RTS_CUDA(cudaMemcpy(&bad, scratch, 8, cudaMemcpyDeviceToHost));
+    if (bad) throw rts::Error(RTS_ERR_PARSE, p + ": area table or sample does not match the sorted values");
+    if (rts::count_fv_mismatches(ctx->cols[column], h.n, d_start, (int)h.K, b->fv, h.fv_stride, scratch,
+                                 ctx->sm_count, 0))
+      throw rts::Error(RTS_ERR_PARSE, p + ": filter vectors do not match column " + std::to_string(column));
     if (ctx->bindex.size() < ctx->cols.size()) ctx->bindex.resize(ctx->cols.size());
     ctx->bindex[column] = std::move(b);
-    ctx->launches += 5;
+    ctx->launches += 6;  // three checksums, the order check, the tables, the filter vectors
     return RTS_OK;
   } catch (const rts::Error &e) {
     return rts::fail(ctx, e.code, e.what());

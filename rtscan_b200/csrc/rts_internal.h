@@ -115,6 +115,11 @@ void launch_bitmap_op(int op, uint32_t *dst, const uint32_t *a, const uint32_t *
                       uint32_t value, int sm_count, cudaStream_t s);
 void launch_bitmap_count(const uint32_t *bm, uint64_t nbits, unsigned long long *count, int sm_count,
                          cudaStream_t s);
+// Loads onto the current device every kernel that a separate-pass scan of
+// single-term passes launches (fused one-term scans, aligned or not, the
+// bitmap AND, the count, the fill), which CUDA's lazy module loading would
+// otherwise load, allocating device memory, at their first launch.
+cudaError_t preload_separate_scan_kernels();
 void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count,
                        int sm_count, cudaStream_t s);
 
@@ -133,6 +138,11 @@ struct GpuBinDex {
   ~GpuBinDex();
 };
 constexpr int kSampleStride = 1024;
+// Filter-vector words of an index (K start values on the device, K-1
+// vectors of fv_stride words) that differ from the ones the start values
+// give for the column: 0 for a consistent index.  Synchronises stream s.
+uint64_t count_fv_mismatches(const uint32_t *col, uint64_t n, const uint32_t *d_start, int K, const uint32_t *fv,
+                             uint64_t fv_stride, unsigned long long *d_bad, int sm_count, cudaStream_t s);
 std::unique_ptr<GpuBinDex> build_bindex(const uint32_t *col, uint64_t n, int K, int sm_count,
                                         cudaStream_t s);
 // Conjunctive query through the column indexes (all referenced columns

@@ -1,5 +1,7 @@
 """GPU BinDex: index contents against the oracle's restated BinDex, and
 query results (sieve mode and candidate mode) against the scalar filter."""
+import struct
+
 import numpy as np
 import pytest
 
@@ -160,3 +162,87 @@ def test_loading_rejects_other_columns_and_damage(ctx, tmp_path):
     ctx.load_columns([a[:-5]])                   # a table of another size
     with pytest.raises(R.RtsError):
         ctx.load_bindex(0, str(f))
+
+
+C1, C2, C3 = np.uint64(0x9E3779B97F4A7C15), np.uint64(0xBF58476D1CE4E5B9), np.uint64(0x94D049BB133111EB)
+
+
+def np_checksum(words):
+    """The file format's checksum (order-dependent sum of a 64-bit mix of
+    (index, word) over 32-bit words), restated with wrapping numpy uint64."""
+    w = np.asarray(words).view(np.uint32).astype(np.uint64)
+    i = np.arange(len(w), dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = w + (i + np.uint64(1)) * C1
+        z = (z ^ (z >> np.uint64(30))) * C2
+        z = (z ^ (z >> np.uint64(27))) * C3
+        z = z ^ (z >> np.uint64(31))
+    return int(np.sum(z, dtype=np.uint64))
+
+
+def split_index_file(raw):
+    """Header fields and the six payload arrays of a BinDex file."""
+    K, n, stride, ns = struct.unpack_from("<IQQQ", raw, 12)
+    lo, hi = struct.unpack_from("<II", raw, 40)
+    off = 112
+    arrays = []
+    for dtype, count in (("<u4", K), ("<u8", K), ("<u4", ns), ("<u4", n), ("<u4", n), ("<u4", (K - 1) * stride)):
+        a = np.frombuffer(raw, dtype=dtype, count=count, offset=off).copy()
+        off += a.nbytes
+        arrays.append(a)
+    return {"K": K, "n": n, "stride": stride, "min": lo, "max": hi}, arrays
+
+
+def join_index_file(raw, fields, arrays):
+    """The file with the given arrays and min/max and every checksum
+    recomputed, so that only the loader's consistency checks can refuse it."""
+    head = bytearray(raw[:112])
+    struct.pack_into("<II", head, 40, fields["min"], fields["max"])
+    for k, a in enumerate(arrays):
+        struct.pack_into("<Q", head, 56 + 8 * k, np_checksum(a))
+    struct.pack_into("<Q", head, 104, np_checksum(np.frombuffer(bytes(head[:104]), dtype="<u4")))
+    return bytes(head) + b"".join(a.tobytes() for a in arrays)
+
+
+@pytest.mark.parametrize("damage", ["rank", "rank_past_n", "start", "sample", "fv_bit", "fv_padding", "min"])
+def test_loading_refuses_consistent_checksums_over_wrong_tables(ctx, tmp_path, damage):
+    """A file whose checksums all agree but whose area table, sample, filter
+    vectors or min/max disagree with its sorted values (a faulty writer or a
+    crafted file) is refused with RTS_ERR_PARSE, and the untouched file still
+    loads and answers exactly."""
+    n, K = 200_003, 16
+    col = D.zipf(n, 51, 1.3)
+    ctx.load_columns([col])
+    ctx.build_bindex(0, K)
+    f = tmp_path / "a.bdx"
+    ctx.save_bindex(0, str(f))
+    raw = f.read_bytes()
+    fields, arrays = split_index_file(raw)
+    assert join_index_file(raw, fields, arrays) == raw  # the restated checksums are the file's
+    start, rank, sample, sval, spos, fv = arrays
+    if damage == "rank":
+        rank[5] += 1
+    elif damage == "rank_past_n":
+        rank[K - 1] = n + 1000
+    elif damage == "start":
+        start[7] += 1
+    elif damage == "sample":
+        sample[3] ^= 1
+    elif damage == "fv_bit":
+        fv[3 * fields["stride"] + 100] ^= 1 << 9
+    elif damage == "fv_padding":
+        words = (n + 31) // 32
+        assert fields["stride"] > words
+        fv[2 * fields["stride"] + words] = 1
+    else:
+        fields["min"] += 1
+    bad = tmp_path / "bad.bdx"
+    bad.write_bytes(join_index_file(raw, fields, arrays))
+    with pytest.raises(R.RtsError) as e:
+        ctx.load_bindex(0, str(bad))
+    assert e.value.code == -5
+    ctx.load_bindex(0, str(f))
+    q = [(0, 3, 900)]
+    got, cnt = bindex_scan(ctx, q)
+    want, wcnt = expect([col], q)
+    assert cnt == wcnt and np.array_equal(got, want)
