@@ -377,15 +377,21 @@ RTS_API rts_status rts_scan_aggregate_async(rts_ctx *ctx, const rts_term *terms,
  * rts_scan_separate_async without a context and without allocating: plain
  * device column pointers in (`ncols` columns of `nrows` values on the
  * current device), caller-owned dev_bitmap (rts_bitmap_words(nrows) words)
- * and *dev_count out, asynchronously on `stream`.  Its scratch bitmap is a
- * file-scope __device__ array of RTS_NOALLOC_MAX_ROWS/8 bytes that every GPU
- * loading this library holds until the process exits; nrows above
- * RTS_NOALLOC_MAX_ROWS is rejected with RTS_ERR_ARG.  The first call on a
- * device looks up that array's device address (once per device, with the
- * device current), so make it before capturing any stream.  Every call
- * shares the one array and the array keeps the last call's contents: the
- * scan overwrites the words it reads, but calls that overlap on the GPU
- * (different streams, or several host threads) race on it. */
+ * and *dev_count out (required here, unlike rts_scan_separate_async),
+ * asynchronously on `stream`.  Its scratch bitmap is a file-scope
+ * __device__ array of RTS_NOALLOC_MAX_ROWS/8 bytes; nrows above
+ * RTS_NOALLOC_MAX_ROWS is rejected with RTS_ERR_ARG.
+ * Set-up: the first call on a device, with that device current, has the
+ * CUDA runtime place the array and the kernels this call launches on the
+ * device (the runtime allocates that memory then; device code loads
+ * lazily) and looks up the array's device address.  From then on the
+ * device holds them until the process exits and no call allocates.  So
+ * make one warm-up call per device before reserving a pool that takes the
+ * rest of the device, and before capturing any stream; a set-up that fails
+ * returns RTS_ERR_CUDA and is retried by the next call.
+ * Every call shares the one array and the array keeps the last call's
+ * contents: the scan overwrites the words it reads, but calls that overlap
+ * on the GPU (different streams, or several host threads) race on it. */
 RTS_API rts_status rts_scan_separate_noalloc_async(const uint32_t *const *dev_cols, int32_t ncols,
                                                    uint64_t nrows, const rts_term *terms, int32_t nterms,
                                                    uint32_t *dev_bitmap, uint64_t *dev_count, void *stream);

@@ -8,12 +8,22 @@
 // latency-critical path, where cudaMalloc's implicit device-wide
 // synchronisation would stall every other stream.  For them this entry
 // point takes plain device pointers (no context) and keeps its scratch
-// bitmap in a fixed file-scope __device__ array, which every GPU that loads
-// the library holds until the process exits.
+// bitmap in a fixed file-scope __device__ array.
+//
+// The CUDA runtime loads device code lazily: the array (16 MiB) and the
+// kernels this entry point launches are placed on a device, in memory the
+// runtime allocates, when the first call on that device sets up (it looks
+// up the array's address and loads the kernels).  From then on the device
+// holds them until the process exits and no call allocates.  A caller that
+// will later hand all of HBM to its own pool therefore makes one warm-up
+// call per device before reserving the pool (and before any stream
+// capture).  A set-up that fails, for instance because the device is
+// already full, is reported and retried by the next call.
 #include <cuda_runtime.h>
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -28,27 +38,36 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];
 
 constexpr int kMaxDevices = 64;
 struct DeviceSetup {
-  std::once_flag once;
+  std::mutex mu;
+  std::atomic<bool> ready{false};
   uint32_t *scratch = nullptr;  // device address of g_noalloc_scratch on this device
   int sm_count = 0;
-  cudaError_t err = cudaSuccess;
 };
 DeviceSetup g_setup[kMaxDevices];
 
-// Once per device, with that device current: the device address of the
-// scratch array (its host-side name is not a device address) and the SM
-// count used to size grids.
-DeviceSetup &setup_for(int dev) {
+// Set-up of the current device `dev`, done by its first successful call:
+// the device address of the scratch array (its host-side name is not a
+// device address), the SM count used to size grids, and the kernels the
+// scan launches loaded onto the device.  Nothing is recorded on failure.
+cudaError_t setup_for(int dev, DeviceSetup *&out) {
   DeviceSetup &d = g_setup[dev];
-  std::call_once(d.once, [&] {
-    void *p = nullptr;
-    d.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (d.err == cudaSuccess) {
-      d.scratch = static_cast<uint32_t *>(p);
-      d.err = cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
-    }
-  });
-  return d;
+  out = &d;
+  if (d.ready.load(std::memory_order_acquire)) return cudaSuccess;
+  std::lock_guard<std::mutex> lk(d.mu);
+  if (d.ready.load(std::memory_order_relaxed)) return cudaSuccess;
+  void *p = nullptr;
+  int sms = 0;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = rts::preload_separate_scan_kernels();
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear it: the next call tries again
+    return e;
+  }
+  d.scratch = static_cast<uint32_t *>(p);
+  d.sm_count = sms;
+  d.ready.store(true, std::memory_order_release);
+  return cudaSuccess;
 }
 
 bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
@@ -90,9 +109,12 @@ rts_status scan_separate_noalloc(const uint32_t *const *dev_cols, int32_t ncols,
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return set_thread_error(RTS_ERR_NODEV, "no current CUDA device");
-  DeviceSetup &d = setup_for(dev);
-  if (d.err != cudaSuccess)
-    return set_thread_error(RTS_ERR_CUDA, std::string("scratch address: ") + cudaGetErrorString(d.err));
+  DeviceSetup *dp = nullptr;
+  e = setup_for(dev, dp);
+  if (e != cudaSuccess)
+    return set_thread_error(RTS_ERR_CUDA, std::string("set-up of the scratch array and kernels on device ") +
+                                              std::to_string(dev) + ": " + cudaGetErrorString(e));
+  DeviceSetup &d = *dp;
   cudaStream_t s = (cudaStream_t)stream;
   unsigned long long *count = reinterpret_cast<unsigned long long *>(dev_count);
   const uint64_t words = rts::words_for(nrows);

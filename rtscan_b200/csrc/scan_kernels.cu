@@ -284,6 +284,23 @@ void launch_bitmap_count(const uint32_t *bm, uint64_t nbits, unsigned long long 
   bitmap_count_kernel<<<grid_for(nbits >> 5, 16, sm_count), kThreads, 0, s>>>(bm, nbits, vec ? 1 : 0, count);
 }
 
+cudaError_t preload_separate_scan_kernels() {
+  const void *kernels[] = {reinterpret_cast<const void *>(scan_fused_kernel<1, true>),
+                           reinterpret_cast<const void *>(scan_fused_kernel<0, false>),
+                           reinterpret_cast<const void *>(bitmap_op_kernel),
+                           reinterpret_cast<const void *>(bitmap_count_kernel),
+                           reinterpret_cast<const void *>(fill_range_kernel),
+                           reinterpret_cast<const void *>(store_count_kernel)};
+  for (const void *k : kernels) {
+    cudaFuncAttributes a;
+    const cudaError_t e = cudaFuncGetAttributes(&a, k);
+    if (e != cudaSuccess) return e;
+  }
+  max_blocks<1, true>(1);  // the occupancy queries that size the fused-scan grids, cached here
+  max_blocks<0, false>(1);
+  return cudaSuccess;
+}
+
 void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count, int sm_count,
                        cudaStream_t s) {
   uint64_t words = (nrows + 31) >> 5;
