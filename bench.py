@@ -591,6 +591,8 @@ def run(args):
     if wl == "batched":
         line["batch_config"] = ctx.batch_config()
         line["batch_config"]["source"] = "autotuned" if tuned else "default"
+        if tuned:
+            line["batch_config"]["autotune"] = ctx.autotune_report()
     line.update(extra)
 
     if args.bindex_io and rank == 0:

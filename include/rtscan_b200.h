@@ -274,13 +274,22 @@ typedef struct rts_batch_config {
 } rts_batch_config;
 RTS_API rts_status rts_set_batch_config(rts_ctx *ctx, const rts_batch_config *cfg);
 RTS_API rts_status rts_get_batch_config(const rts_ctx *ctx, rts_batch_config *cfg);
-/* Time every candidate launch shape on a row sample (up to 2^24 rows) of the
- * resident table with these queries, keep the fastest for this context, and
+/* Time every candidate launch shape on the table's first rows (enough that
+ * the batch's bitmaps take at most a quarter of the free device memory,
+ * between 2^24 and 2^27 rows) with these queries, keep the fastest for this context, and
  * report it in *best (may be NULL).  With a cache_path, a previous result for
  * the same GPU, SM count, column count, table size and batch size is reused
  * and new results are appended. */
 RTS_API rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,
                                       int32_t nqueries, const char *cache_path, rts_batch_config *best);
+/* The last rts_autotune_batch of this context as JSON text: the sample rows,
+ * every candidate shape with its time per call on the sample, the best and
+ * the default shape's times ({"cached": true} when the cache answered; empty
+ * before any tuning).  Copies at most size-1 bytes and a terminating NUL into
+ * buf (may be NULL) and sets *needed (may be NULL) to the full length + 1.
+ * No reference counterpart (its launch shape is fixed at compile time,
+ * Makefile:31-58). */
+RTS_API rts_status rts_autotune_report(const rts_ctx *ctx, char *buf, uint64_t size, uint64_t *needed);
 
 /* ---- serving: continuous batching over resident columns ----------------- */
 /* No reference counterpart (the reference drivers answer one query at a time,

@@ -136,6 +136,7 @@ _SIGS = [
     ("rts_get_batch_config", ctypes.c_int32, [_P, ctypes.POINTER(BatchConfig)]),
     ("rts_autotune_batch", ctypes.c_int32, [_P, _TERMP, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
                                             ctypes.c_char_p, ctypes.POINTER(BatchConfig)]),
+    ("rts_autotune_report", ctypes.c_int32, [_P, ctypes.c_char_p, ctypes.c_uint64, _U64P]),
     ("rts_server_start", ctypes.c_int32, [_P, ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
     ("rts_server_submit", ctypes.c_int32, [_P, _TERMP, ctypes.c_int32, _U64P]),
     ("rts_server_poll", ctypes.c_int32, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32), _U64P]),
@@ -551,6 +552,16 @@ class Context:
         self._c(lib().rts_autotune_batch(self._h, arr, off, len(queries),
                                          cache_path.encode() if cache_path else None, ctypes.byref(c)))
         return c.as_dict()
+
+    def autotune_report(self) -> dict:
+        """Every candidate of the last autotune_batch with its time per call
+        on the sample, the best and the default shape's times."""
+        import json
+        need = ctypes.c_uint64(0)
+        self._c(lib().rts_autotune_report(self._h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(max(1, need.value))
+        self._c(lib().rts_autotune_report(self._h, buf, need.value, None))
+        return json.loads(buf.value.decode()) if buf.value else {}
 
     def bitmap_op_async(self, op: int, dst: int, a: int, b: int, words: int, value: int = 0, stream: int = 0):
         self._c(lib().rts_bitmap_op_async(self._h, op, dst, a, b, words, value, stream))

@@ -206,6 +206,7 @@ struct rts_ctx {
   rts::BatchScratch *batch = nullptr;
   rts::HostBatchBuffers *host_batch = nullptr;
   rts::BatchConfig batch_cfg;
+  std::string tune_report;  // JSON of the last rts_autotune_batch (rts_autotune_report)
   std::unique_ptr<rts::EncodeMap> encode;  // set by rts_encode_table
   std::atomic<uint64_t> launches{0};
   std::string err;

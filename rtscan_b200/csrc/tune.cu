@@ -8,6 +8,14 @@
 // every candidate on a row sample of the resident table with the caller's
 // queries, keeps the fastest, and can cache the choice in a small text file
 // keyed by GPU, SM count, column count, table size and batch size.
+//
+// Candidates: variant 4 (one 16-warp CTA per SM, pass shapes of 128/256/512
+// slots) at seven pass sizes from 128 to 512 queries and two table budgets,
+// and variant 3 at 8 and 16 warps per CTA with two budgets each.  The sample
+// is the table's first rows: as many as the result bitmaps of the batch fit
+// in a quarter of the free device memory, at least 2^24 and at most 2^27
+// (all of a smaller table).  Each candidate runs once untimed and twice
+// timed; the report (rts_autotune_report) lists every candidate's time.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -26,10 +34,14 @@ struct Candidate {
   size_t budget;
 };
 
-const Candidate kCandidates[] = {
-    {4, 16, 512, 136 * 1024}, {4, 16, 384, 136 * 1024}, {4, 16, 256, 96 * 1024},
-    {3, 16, 256, 88 * 1024},  {3, 16, 256, 64 * 1024},  {3, 8, 256, 40 * 1024}, {3, 8, 256, 140 * 1024},
-};
+std::vector<Candidate> candidates() {
+  std::vector<Candidate> c;
+  for (int qpp : {512, 448, 384, 320, 256, 192, 128})
+    for (size_t budget : {(size_t)136 * 1024, (size_t)112 * 1024}) c.push_back({4, 16, qpp, budget});
+  for (size_t budget : {(size_t)88 * 1024, (size_t)64 * 1024}) c.push_back({3, 16, 256, budget});
+  for (size_t budget : {(size_t)140 * 1024, (size_t)40 * 1024}) c.push_back({3, 8, 256, budget});
+  return c;
+}
 
 size_t max_budget(int variant, int warps) {
   if (variant == 4) return 136 * 1024;
@@ -127,6 +139,7 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
   rts::BatchConfig cached;
   if (cache_lookup(cache_path, key, &cached)) {
     ctx->batch_cfg = cached;
+    ctx->tune_report = "{\"cached\": true}";
     if (best_out) rts_get_batch_config(ctx, best_out);
     return RTS_OK;
   }
@@ -138,8 +151,12 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
   rts_status rc = RTS_OK;
   try {
     rts::DeviceGuard device_guard(ctx->device);
-    // tune on a row sample (all of a small table)
-    const uint64_t sample = std::min<uint64_t>(saved_n, 1ull << 24);
+    // tune on the table's first rows: as many as a quarter of the free
+    // memory holds the batch's bitmaps for, within [2^24, 2^27] rows
+    size_t free_b = 0, total_b = 0;
+    RTS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const uint64_t fit = (uint64_t)((double)free_b / 4 / ((double)nq / 8)) & ~4095ull;
+    const uint64_t sample = std::min<uint64_t>(saved_n, std::max<uint64_t>(1ull << 24, std::min<uint64_t>(fit, 1ull << 27)));
     ctx->nrows = sample;
     const uint64_t stride = (rts::words_for(sample) + 31) / 32 * 32;
     if (cudaMalloc(&bm, (size_t)nq * stride * 4) != cudaSuccess || cudaMalloc(&cnt, (size_t)nq * 8) != cudaSuccess) {
@@ -150,7 +167,12 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
     RTS_CUDA(cudaEventCreate(&e1));
     double best_ms = 1e300;
     rts::BatchConfig best = saved_cfg;
-    for (const Candidate &c : kCandidates) {
+    std::string report = "{\"sample_rows\": " + std::to_string(sample) + ", \"queries\": " + std::to_string(nq) +
+                         ", \"candidates\": [";
+    const rts::BatchConfig dflt;
+    double default_ms = -1;
+    bool first = true;
+    for (const Candidate &c : candidates()) {
       ctx->batch_cfg.variant = c.variant;
       ctx->batch_cfg.warps_per_cta = c.warps;
       ctx->batch_cfg.max_queries_per_pass = c.qpp;
@@ -162,11 +184,23 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
       RTS_CUDA(cudaEventSynchronize(e1));
       float ms = 0;
       RTS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      char item[160];
+      snprintf(item, sizeof item, "%s{\"variant\": %d, \"warps_per_cta\": %d, \"max_queries_per_pass\": %d, "
+               "\"table_budget_bytes\": %zu, \"ms\": %.4f}", first ? "" : ", ", c.variant, c.warps, c.qpp, c.budget,
+               ms / 2);
+      report += item;
+      first = false;
+      if (c.variant == dflt.variant && c.warps == dflt.warps_per_cta && c.qpp == dflt.max_queries_per_pass &&
+          c.budget == dflt.table_budget)
+        default_ms = ms / 2;
       if (ms / 2 < best_ms) {
         best_ms = ms / 2;
         best = ctx->batch_cfg;
       }
     }
+    char tail[160];
+    snprintf(tail, sizeof tail, "], \"best_ms\": %.4f, \"default_ms\": %.4f}", best_ms, default_ms);
+    ctx->tune_report = report + tail;
     ctx->batch_cfg = best;
     ctx->nrows = saved_n;
     cache_store(cache_path, key, best, best_ms);
@@ -182,6 +216,18 @@ rts_status rts_autotune_batch(rts_ctx *ctx, const rts_term *terms, const int32_t
   if (e1) cudaEventDestroy(e1);
   if (rc == RTS_OK && best_out) rts_get_batch_config(ctx, best_out);
   return rc;
+}
+
+rts_status rts_autotune_report(const rts_ctx *ctx, char *buf, uint64_t size, uint64_t *needed) {
+  if (!ctx) return rts::set_thread_error(RTS_ERR_ARG, "null context");
+  const std::string &r = ctx->tune_report;
+  if (needed) *needed = r.size() + 1;
+  if (buf && size) {
+    const size_t m = std::min<size_t>(r.size(), size - 1);
+    memcpy(buf, r.data(), m);
+    buf[m] = '\0';
+  }
+  return RTS_OK;
 }
 
 }  // extern "C"

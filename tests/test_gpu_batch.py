@@ -216,6 +216,54 @@ def test_autotune_picks_a_valid_shape_and_caches_it(ctx, tmp_path):
         ctx.set_batch_config(4, 16, 513, 88 * 1024)
 
 
+def test_autotuned_shape_is_not_slower_than_the_default(ctx):
+    """The tuner searches pass sizes, table budgets, variants and warps per
+    CTA on a sample of the real table, reports every candidate, and its
+    choice, timed again on the whole table after tuning, is no slower than
+    the default shape beyond timing noise (5 %)."""
+    n = 1 << 25
+    cols = [D.zipf(n, 220, 1.1), D.zipf(n, 221, 1.5), D.normal(n, 222), D.zipf(n, 223, 1.3)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 1024, seed=8)
+    old = ctx.batch_config()
+    try:
+        ctx.set_batch_config(4, 16, 512, 136 * 1024)
+        best = ctx.autotune_batch(qs)
+        rep = ctx.autotune_report()
+        assert rep["sample_rows"] == n and rep["queries"] == len(qs)
+        shapes = {(c["variant"], c["warps_per_cta"], c["max_queries_per_pass"], c["table_budget_bytes"])
+                  for c in rep["candidates"]}
+        assert len(shapes) == len(rep["candidates"]) >= 18
+        assert {v for v, _, _, _ in shapes} == {3, 4} and {w for _, w, _, _ in shapes} == {8, 16}
+        assert rep["best_ms"] <= rep["default_ms"]
+        words = R.bitmap_words(n)
+        stride = (words + 31) // 32 * 32
+        out = torch.empty(len(qs) * stride, dtype=torch.int32, device="cuda")
+        cnt = torch.empty(len(qs), dtype=torch.int64, device="cuda")
+        s = torch.cuda.current_stream()
+
+        def med(reps=5):
+            pq = R.prepare(qs)
+            ctx.scan_batch_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s.cuda_stream)
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                ctx.scan_batch_async(pq, out.data_ptr(), stride, cnt.data_ptr(), s.cuda_stream)
+                e1.record(s)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return sorted(ts)[reps // 2]
+
+        tuned = med()
+        ctx.set_batch_config(4, 16, 512, 136 * 1024)
+        default = med()
+        assert tuned <= default * 1.05, (best, tuned, default)
+    finally:
+        ctx.set_batch_config(old["variant"], old["warps_per_cta"], old["max_queries_per_pass"],
+                             old["table_budget_bytes"])
+
+
 @pytest.mark.parametrize("n,nq", [(70_001, 300), (9_000_011, 300), (9_000_011, 20), (9_000_011, 2),
                                   (9_000_011, 1)])
 def test_batch_host_buffers(ctx, n, nq):
