@@ -686,6 +686,25 @@ def event_median(torch, fn, reps=9, warm=3):
     return statistics.median(ts)
 
 
+def stream_per_call(torch, fn, calls=20, reps=5):
+    """Device time (ms) per call of fn() issued `calls` times back to back
+    between two CUDA events (host planning overlaps the device work, as in
+    a stream of queries), median over `reps` such runs."""
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        fn()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(calls):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / calls)
+    return statistics.median(ts)
+
+
 def single_leg(torch, R, D, dev, n, hbm_peak):
     """The plain single-query scan: one uniform 2^32 column of n rows, one
     range at 10 % selectivity ([q45, q55] of a sample), one fused-scan launch.
@@ -761,8 +780,11 @@ def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
     scan and through the BinDex (built once per column, K areas), bitmaps
     compared: a uniform 2^32 column at 0.1/1/10/50/90 % (bounds at sample
     quantiles) and columns of 256 and 64 distinct values (central value runs
-    nearest those shares; the achieved selectivity is reported).  Fused
-    bytes: 4N + N/8.  BinDex bytes are those of the plan its planner picks,
+    nearest those shares; the achieved selectivity is reported).  Times are
+    the device time per query in a stream of 20 back-to-back calls (`_us`,
+    the basis of GB/s and frac) and the latency of one call alone
+    (`_latency_us`, which includes the host's planning and launch of that
+    call while the device waits).  Fused bytes: 4N + N/8.  BinDex bytes are those of the plan its planner picks,
     from exact ranks, costed as bindex_query (csrc/bindex.cu) costs it: the
     result write, every filter vector read, and 12 B per re-tested row (its
     row id, its gathered value and its result word); a query whose matches
@@ -819,16 +841,20 @@ def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
             cand_cost = n / 8 + (match + 2048) * 40.0
             refine_only = cand_cost < sieve_cost
             nbytes = n / 8 + match * 12 if refine_only else n / 8 * (1 + fv_reads) + refine * 12
-            t_b = event_median(torch, lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream),
-                               reps=7)
+            bq = lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream)
+            fq = lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream)
+            lat_b = event_median(torch, bq, reps=7)
+            t_b = stream_per_call(torch, bq)
             hits = int(cnt.item())
-            t_f = event_median(torch, lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream),
-                               reps=7)
+            lat_f = event_median(torch, fq, reps=7)
+            t_f = stream_per_call(torch, fq)
             fgbs = fused_bytes / (t_f * 1e-3) / 1e9
             res["queries"].append({
                 "column": kind, "target": sel, "lo": lo, "hi": hi, "selectivity": round(hits / n, 5),
-                "fused_us": round(t_f * 1e3, 1), "fused_GB_s": round(fgbs, 1), "fused_frac": round(fgbs / hbm_peak, 4),
-                "bindex_us": round(t_b * 1e3, 1), "bindex_rows_per_s": round(n / (t_b * 1e-3), 1),
+                "fused_us": round(t_f * 1e3, 1), "fused_latency_us": round(lat_f * 1e3, 1),
+                "fused_GB_s": round(fgbs, 1), "fused_frac": round(fgbs / hbm_peak, 4),
+                "bindex_us": round(t_b * 1e3, 1), "bindex_latency_us": round(lat_b * 1e3, 1),
+                "bindex_rows_per_s": round(n / (t_b * 1e-3), 1),
                 "bindex_plan": "refine_only" if refine_only else "sieve",
                 "bindex_refined_rows": match if refine_only else refine, "bindex_bytes_MB": round(nbytes / 1e6, 2),
                 "bindex_GB_s": round(nbytes / (t_b * 1e-3) / 1e9, 1),

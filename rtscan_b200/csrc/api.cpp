@@ -117,7 +117,7 @@ void fused(rts_ctx *ctx, const Plan &plan, uint32_t *out, unsigned long long *co
   const uint64_t n = ctx->nrows;
   if (plan.empty || plan.terms.empty()) {
     rts::launch_fill_range(out, n, !plan.empty, count, ctx->sm_count, s);
-    check_launch(ctx, count ? 2 : 1);
+    check_launch(ctx, 1);
     return;
   }
   if (count) RTS_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned long long), s));
@@ -184,6 +184,7 @@ rts_ctx::~rts_ctx() {
   if (plan_dev) cudaFree(plan_dev);
   if (plan_host) cudaFreeHost(plan_host);
   if (small_dev) cudaFree(small_dev);
+  if (query_slots) cudaFree(query_slots);
   if (agg_dev) cudaFree(agg_dev);
   if (batch) rts::destroy_batch(batch);
   if (host_batch) rts::destroy_host_batch(host_batch);

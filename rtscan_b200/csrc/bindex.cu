@@ -42,6 +42,7 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kThreads = 256;
 constexpr int kMaxBounds = 2 * kFusedMaxTerms;
+constexpr uint64_t kRefineInSieveRows = 1024;  // estimated refine rows the sieve's last block takes
 
 // First index i in [lo, hi) with a[i] >= b, else hi (a sorted ascending).
 // Called by a whole warp; every lane returns the same value.
@@ -158,78 +159,15 @@ void launch_fv(const uint32_t *col, uint64_t n, const uint32_t *start, int K, ui
 }
 
 // ---- query -------------------------------------------------------------------
-
-struct SieveTerm {
-  const uint32_t *U;  // upper-bound approximation (x < b_hi); null = constant
-  const uint32_t *L;  // lower-bound approximation (x < b_lo); null = constant
-  uint32_t u_const;   // value of U when null (0 or ~0)
-  uint32_t l_const;   // value of L when null
-};
-
-struct SieveParams {
-  SieveTerm t[kFusedMaxTerms];
-  int nterms;
-  uint32_t *out;
-  unsigned long long *count;
-  uint64_t words;
-  uint32_t tail_mask;  // mask of the last word (rows past n are zero)
-  int vec;
-};
-
-__device__ __forceinline__ uint32_t sieve_word(const SieveParams &p, uint64_t w) {
-  uint32_t r = 0xFFFFFFFFu;
-  for (int t = 0; t < p.nterms; t++) {
-    const SieveTerm &s = p.t[t];
-    const uint32_t u = s.U ? __ldg(s.U + w) : s.u_const;
-    const uint32_t l = s.L ? __ldg(s.L + w) : s.l_const;
-    r &= u & ~l;
-  }
-  return r;
-}
-
-__device__ __forceinline__ uint4 ld4(const uint32_t *p, uint64_t i4) {
-  return __ldg(reinterpret_cast<const uint4 *>(p) + i4);
-}
-
-__global__ void __launch_bounds__(kThreads) sieve_kernel(const __grid_constant__ SieveParams p) {
-  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint32_t cnt = 0;
-  uint64_t done = 0;
-  if (p.vec) {
-    const uint64_t nv = (p.words - 1) / 4;  // vectors entirely before the last word
-    for (uint64_t i = tid; i < nv; i += stride) {
-      uint4 r = make_uint4(~0u, ~0u, ~0u, ~0u);
-      for (int t = 0; t < p.nterms; t++) {
-        const SieveTerm &s = p.t[t];
-        uint4 u = s.U ? ld4(s.U, i) : make_uint4(s.u_const, s.u_const, s.u_const, s.u_const);
-        uint4 l = s.L ? ld4(s.L, i) : make_uint4(s.l_const, s.l_const, s.l_const, s.l_const);
-        r.x &= u.x & ~l.x;
-        r.y &= u.y & ~l.y;
-        r.z &= u.z & ~l.z;
-        r.w &= u.w & ~l.w;
-      }
-      reinterpret_cast<uint4 *>(p.out)[i] = r;
-      cnt += __popc(r.x) + __popc(r.y) + __popc(r.z) + __popc(r.w);
-    }
-    done = nv * 4;
-  }
-  for (uint64_t w = done + tid; w < p.words; w += stride) {
-    uint32_t r = sieve_word(p, w);
-    if (w == p.words - 1) r &= p.tail_mask;
-    p.out[w] = r;
-    cnt += __popc(r);
-  }
-  __shared__ unsigned long long part[kThreads / 32];
-  cnt = __reduce_add_sync(kFull, cnt);
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = cnt;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long s = 0;
-    for (int i = 0; i < kThreads / 32; i++) s += part[i];
-    if (s) atomicAdd(p.count, s);
-  }
-}
+//
+// A query is two launches on the caller's stream: the sieve kernel writes
+// every result word once (U & ~L over terms, or zeros in candidate mode)
+// while one warp of its first block per refine range resolves the range's
+// ends (warp searches in the sorted values, latency hidden behind the
+// streaming); its blocks sum their popcounts into a context slot and the
+// last block to finish (an arrival ticket, no waiting) stores the count.
+// The refine kernel then reads the resolved ranges from the slot, re-tests
+// their rows and corrects the bits and the count with atomics.
 
 // A refine range end: a known sorted rank, or the lower bound of `b` in the
 // sorted values, searched in [wlo, whi].
@@ -247,58 +185,230 @@ struct RefineRange {
   int term;  // the term on this range's column (its value is sval[i])
 };
 
-struct RefineParams {
-  DevTerm t[kFusedMaxTerms];
-  int nterms;
-  RefineRange r[kMaxBounds];
-  int nranges;
+}  // namespace
+
+// Context memory shared by the two launches of one query (kQuerySlots of
+// them, used in turn, so queries on different streams do not share one):
+// the resolved refine ranges, and the sieve's running count and finished
+// blocks, both zero between queries.
+struct QuerySlot {
+  unsigned long long acc;
+  unsigned int ticket;
+  unsigned int pad;
+  unsigned long long begin[kMaxBounds], end[kMaxBounds];
+};
+
+namespace {
+
+struct SieveTerm {
+  const uint32_t *U;  // upper-bound approximation (x < b_hi); null = constant
+  const uint32_t *L;  // lower-bound approximation (x < b_lo); null = constant
+  uint32_t u_const;   // value of U when null (0 or ~0)
+  uint32_t l_const;   // value of L when null
+};
+
+struct SieveParams {
+  SieveTerm t[kFusedMaxTerms];
+  int nterms;         // 0: candidate mode, every word zero
   uint32_t *out;
   unsigned long long *count;
+  uint64_t words;
+  uint32_t tail_mask;  // mask of the last word (rows past n are zero)
+  int vec;
+  QuerySlot *slot;
+  RefineRange r[kMaxBounds];  // the refine ranges whose ends block 0 resolves
+  int nranges;
+  // small refine sets: the last block to finish (every word written by
+  // then) re-tests them here and no refine launch follows
+  int refine_here;
+  int zero_start;
+  DevTerm rt[kFusedMaxTerms];
+  int rnterms;
 };
+
+__device__ __forceinline__ uint32_t sieve_word(const SieveParams &p, uint64_t w) {
+  uint32_t r = 0xFFFFFFFFu;
+  for (int t = 0; t < p.nterms; t++) {
+    const SieveTerm &s = p.t[t];
+    const uint32_t u = s.U ? __ldg(s.U + w) : s.u_const;
+    const uint32_t l = s.L ? __ldg(s.L + w) : s.l_const;
+    r &= u & ~l;
+  }
+  return p.nterms ? r : 0u;
+}
+
+__device__ __forceinline__ uint4 ld4(const uint32_t *p, uint64_t i4) {
+  return __ldg(reinterpret_cast<const uint4 *>(p) + i4);
+}
 
 __device__ uint64_t resolve_end(const RefineRange &rg, const RangeEnd &e) {
   if (e.kind == 0) return e.rank;
   return warp_lower_bound(rg.sval, e.wlo, e.whi, e.b);
 }
 
+// Re-test the rows of the refine ranges (ends begin[r], end[r]) that fall to
+// thread `tid` of `stride`, set or clear their bits; returns the change of
+// the count.  Two rows per iteration: their loads (row id, own value,
+// gathers) are issued before either row's test and atomic.
+__device__ long long refine_rows(const RefineRange *ranges, int nranges, const DevTerm *terms, int nterms,
+                                 const unsigned long long *begin, const unsigned long long *end, uint64_t tid,
+                                 uint64_t stride, bool zero_start, uint32_t *out) {
+  long long delta = 0;
+  auto apply = [&](uint32_t row, bool hit) {
+    const uint32_t bit = 1u << (31 - (row & 31));
+    uint32_t *word = out + (row >> 5);
+    if (hit) {
+      const uint32_t old = atomicOr(word, bit);
+      delta += (old & bit) ? 0 : 1;
+    } else if (!zero_start) {  // in candidate mode the bit is still zero
+      const uint32_t old = atomicAnd(word, ~bit);
+      delta -= (old & bit) ? 1 : 0;
+    }
+  };
+  for (int r = 0; r < nranges; r++) {
+    const RefineRange &rg = ranges[r];
+    const uint64_t e = end[r];
+    for (uint64_t i = begin[r] + tid; i < e; i += 2 * stride) {
+      const uint64_t i2 = i + stride;
+      const bool two = i2 < e;
+      const uint32_t row = __ldg(rg.spos + i), own = __ldg(rg.sval + i);
+      const uint32_t row2 = two ? __ldg(rg.spos + i2) : row, own2 = two ? __ldg(rg.sval + i2) : own;
+      bool hit = true, hit2 = true;
+      for (int t = 0; t < nterms; t++) {
+        const bool mine = t == rg.term;
+        const uint32_t x = mine ? own : __ldg(terms[t].col + row);
+        const uint32_t x2 = mine ? own2 : __ldg(terms[t].col + row2);
+        hit = hit && x - terms[t].lo <= terms[t].span;
+        hit2 = hit2 && x2 - terms[t].lo <= terms[t].span;
+      }
+      apply(row, hit);
+      if (two) apply(row2, hit2);
+    }
+  }
+  return delta;
+}
+
+__global__ void __launch_bounds__(kThreads) sieve_kernel(const __grid_constant__ SieveParams p) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (blockIdx.x == 0) {
+    for (int r = warp; r < p.nranges; r += kThreads / 32) {
+      const uint64_t a = resolve_end(p.r[r], p.r[r].e0);
+      const uint64_t b = resolve_end(p.r[r], p.r[r].e1);
+      if (lane == 0) {
+        p.slot->begin[r] = min(a, b);
+        p.slot->end[r] = max(a, b);
+      }
+    }
+  }
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint32_t cnt = 0;
+  uint64_t done = 0;
+  if (p.vec) {
+    const uint64_t nv = (p.words - 1) / 4;  // vectors entirely before the last word
+    // two vectors per iteration: each thread keeps the loads of both in flight
+    for (uint64_t i = tid; i < nv; i += 2 * stride) {
+      const uint64_t i2 = i + stride;
+      const bool two = i2 < nv;
+      uint4 r = make_uint4(0, 0, 0, 0), r2 = r;
+      if (p.nterms) {
+        r = r2 = make_uint4(~0u, ~0u, ~0u, ~0u);
+        for (int t = 0; t < p.nterms; t++) {
+          const SieveTerm &s = p.t[t];
+          const uint4 cu = make_uint4(s.u_const, s.u_const, s.u_const, s.u_const);
+          const uint4 cl = make_uint4(s.l_const, s.l_const, s.l_const, s.l_const);
+          const uint4 u = s.U ? ld4(s.U, i) : cu;
+          const uint4 l = s.L ? ld4(s.L, i) : cl;
+          const uint4 u2 = (s.U && two) ? ld4(s.U, i2) : cu;
+          const uint4 l2 = (s.L && two) ? ld4(s.L, i2) : cl;
+          r.x &= u.x & ~l.x;
+          r.y &= u.y & ~l.y;
+          r.z &= u.z & ~l.z;
+          r.w &= u.w & ~l.w;
+          r2.x &= u2.x & ~l2.x;
+          r2.y &= u2.y & ~l2.y;
+          r2.z &= u2.z & ~l2.z;
+          r2.w &= u2.w & ~l2.w;
+        }
+        cnt += __popc(r.x) + __popc(r.y) + __popc(r.z) + __popc(r.w);
+        if (two) cnt += __popc(r2.x) + __popc(r2.y) + __popc(r2.z) + __popc(r2.w);
+      }
+      reinterpret_cast<uint4 *>(p.out)[i] = r;
+      if (two) reinterpret_cast<uint4 *>(p.out)[i2] = r2;
+    }
+    done = nv * 4;
+  }
+  for (uint64_t w = done + tid; w < p.words; w += stride) {
+    uint32_t r = sieve_word(p, w);
+    if (w == p.words - 1) r &= p.tail_mask;
+    p.out[w] = r;
+    cnt += __popc(r);
+  }
+  // the block's popcount into the slot; the last block stores the count
+  __shared__ unsigned long long part[kThreads / 32];
+  cnt = __reduce_add_sync(kFull, cnt);
+  if (lane == 0) part[warp] = cnt;
+  __syncthreads();
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int i = 0; i < kThreads / 32; i++) s += part[i];
+    if (s) atomicAdd(&p.slot->acc, s);
+    __threadfence();
+    s_last = atomicAdd(&p.slot->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  // the last block: every other block's words and popcount are in place
+  __threadfence();
+  long long delta = 0;
+  if (p.refine_here) {
+    __shared__ unsigned long long s_begin[kMaxBounds], s_end[kMaxBounds];
+    for (int r = threadIdx.x; r < p.nranges; r += kThreads) {
+      s_begin[r] = p.slot->begin[r];
+      s_end[r] = p.slot->end[r];
+    }
+    __syncthreads();
+    delta = refine_rows(p.r, p.nranges, p.rt, p.rnterms, s_begin, s_end, threadIdx.x, kThreads, p.zero_start != 0,
+                        p.out);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) delta += __shfl_xor_sync(kFull, delta, o);
+  __syncthreads();
+  if (lane == 0) part[warp] = (unsigned long long)delta;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long d = 0;
+    for (int i = 0; i < kThreads / 32; i++) d += (long long)part[i];
+    *p.count = atomicExch(&p.slot->acc, 0ull) + (unsigned long long)d;
+    p.slot->ticket = 0;
+  }
+}
+
+struct RefineParams {
+  DevTerm t[kFusedMaxTerms];
+  int nterms;
+  RefineRange r[kMaxBounds];
+  int nranges;
+  const QuerySlot *slot;  // the ranges' resolved ends
+  int zero_start;         // candidate mode: every bit starts at zero, so misses write nothing
+  uint32_t *out;
+  unsigned long long *count;
+};
+
 __global__ void __launch_bounds__(kThreads) refine_kernel(const __grid_constant__ RefineParams p) {
   __shared__ unsigned long long s_begin[kMaxBounds], s_end[kMaxBounds];
   __shared__ long long part[kThreads / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r = warp; r < p.nranges; r += kThreads / 32) {
-    const uint64_t a = resolve_end(p.r[r], p.r[r].e0);
-    const uint64_t b = resolve_end(p.r[r], p.r[r].e1);
-    if (lane == 0) {
-      s_begin[r] = min(a, b);
-      s_end[r] = max(a, b);
-    }
+  for (int r = threadIdx.x; r < p.nranges; r += kThreads) {
+    s_begin[r] = p.slot->begin[r];
+    s_end[r] = p.slot->end[r];
   }
   __syncthreads();
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  long long delta = 0;
-  for (int r = 0; r < p.nranges; r++) {
-    const RefineRange &rg = p.r[r];
-    const uint64_t end = s_end[r];
-    for (uint64_t i = s_begin[r] + tid; i < end; i += stride) {
-      const uint32_t row = __ldg(rg.spos + i);
-      const uint32_t own = __ldg(rg.sval + i);
-      bool hit = true;
-      for (int t = 0; t < p.nterms && hit; t++) {
-        const uint32_t x = (t == rg.term) ? own : __ldg(p.t[t].col + row);
-        hit = x - p.t[t].lo <= p.t[t].span;
-      }
-      const uint32_t bit = 1u << (31 - (row & 31));
-      uint32_t *word = p.out + (row >> 5);
-      if (hit) {
-        const uint32_t old = atomicOr(word, bit);
-        delta += (old & bit) ? 0 : 1;
-      } else {
-        const uint32_t old = atomicAnd(word, ~bit);
-        delta -= (old & bit) ? 1 : 0;
-      }
-    }
-  }
+  const long long delta =
+      refine_rows(p.r, p.nranges, p.t, p.nterms, s_begin, s_end, tid, stride, p.zero_start != 0, p.out);
   long long d = delta;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
@@ -568,10 +678,16 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
     return r;
   };
 
+  SieveParams sp;
+  memset(&sp, 0, sizeof sp);
+  sp.out = out;
+  sp.count = count;
+  sp.words = words_for(n);
+  const uint32_t rem = (uint32_t)(n & 31);
+  sp.tail_mask = rem ? ~(0xFFFFFFFFu >> rem) : 0xFFFFFFFFu;
+  sp.vec = ((uintptr_t)out & 15) == 0;
   if (best_cand_cost < sieve_cost) {
     // Candidate mode: start from zero, re-test the matches of one term.
-    launch_fill_range(out, n, false, count, ctx->sm_count, s);
-    launches += 2;
     const int t = best_cand;
     const GpuBinDex &B = *ctx->bindex[tc[t]];
     RefineRange &rg = rp.r[0];
@@ -581,16 +697,9 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
     rg.e0 = tp[t].has_lo ? end_of(tp[t].e_lo, tlo[t]) : end_rank(0);
     rg.e1 = tp[t].has_hi ? end_of(tp[t].e_hi, thi[t] + 1) : end_rank(n);
     rp.nranges = 1;
+    rp.zero_start = 1;
   } else {
-    SieveParams sp;
-    memset(&sp, 0, sizeof sp);
     sp.nterms = T;
-    sp.out = out;
-    sp.count = count;
-    sp.words = words_for(n);
-    const uint32_t rem = (uint32_t)(n & 31);
-    sp.tail_mask = rem ? ~(0xFFFFFFFFu >> rem) : 0xFFFFFFFFu;
-    sp.vec = ((uintptr_t)out & 15) == 0;
     for (int t = 0; t < T; t++) {
       const GpuBinDex &B = *ctx->bindex[tc[t]];
       SieveTerm &st = sp.t[t];
@@ -618,15 +727,39 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
         rg.e1 = end_rank(tp[t].a_lo.rank);
       }
     }
-    RTS_CUDA(cudaMemsetAsync(count, 0, 8, s));
-    const uint64_t nvec = sp.words / 4 + 1;
-    sieve_kernel<<<blocks_for(nvec, ctx->sm_count, 8), kThreads, 0, s>>>(sp);
+  }
+  if (!ctx->query_slots) {
+    if (cudaMalloc(&ctx->query_slots, kQuerySlots * sizeof(QuerySlot)) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(RTS_ERR_NOMEM, "device allocation failed");
+    }
+    RTS_CUDA(cudaMemsetAsync(ctx->query_slots, 0, kQuerySlots * sizeof(QuerySlot), s));
+  }
+  QuerySlot *slot = ctx->query_slots + (ctx->query_next++ % kQuerySlots);
+  sp.slot = slot;
+  sp.nranges = rp.nranges;
+  for (int r = 0; r < rp.nranges; r++) sp.r[r] = rp.r[r];
+  uint64_t est_rows = 0;
+  for (int t = 0; t < T; t++) est_rows += tp[t].refine_est;
+  if (rp.zero_start) est_rows = tp[best_cand].match_est;
+  // A refine set estimated at a few rows (exact ends can differ from the
+  // estimates by a sample stride) costs the sieve's last block less than a
+  // launch of its own.
+  if (est_rows <= kRefineInSieveRows) {
+    sp.refine_here = 1;
+    sp.zero_start = rp.zero_start;
+    sp.rnterms = rp.nterms;
+    for (int t = 0; t < rp.nterms; t++) sp.rt[t] = rp.t[t];
+  }
+  const uint64_t nvec = sp.words / 4 + 1;
+  sieve_kernel<<<blocks_for(nvec, ctx->sm_count, 4), kThreads, 0, s>>>(sp);  // one wave: 48 registers allow 5 blocks per SM
+  launches++;
+  if (rp.nranges && !sp.refine_here) {
+    rp.slot = slot;
+    const uint64_t refine_rows = est_rows;
+    refine_kernel<<<blocks_for(std::max<uint64_t>(refine_rows, 1), ctx->sm_count, 8), kThreads, 0, s>>>(rp);
     launches++;
   }
-  uint64_t refine_rows = 0;
-  for (int t = 0; t < T; t++) refine_rows += tp[t].refine_est;
-  refine_kernel<<<blocks_for(std::max<uint64_t>(refine_rows, 1), ctx->sm_count, 4), kThreads, 0, s>>>(rp);
-  launches++;
   RTS_CUDA(cudaGetLastError());
   ctx->launches += launches;
 }

@@ -138,6 +138,8 @@ struct GpuBinDex {
   ~GpuBinDex();
 };
 constexpr int kSampleStride = 1024;
+struct QuerySlot;                 // context memory of one BinDex query launch (bindex.cu)
+constexpr int kQuerySlots = 64;
 // Filter-vector words of an index (K start values on the device, K-1
 // vectors of fv_stride words) that differ from the ones the start values
 // give for the column: 0 for a consistent index.  Synchronises stream s.
@@ -201,6 +203,8 @@ struct rts_ctx {
   size_t plan_bytes = 0;
   void *plan_host = nullptr;  // pinned
   void *small_dev = nullptr;
+  rts::QuerySlot *query_slots = nullptr;  // BinDex query launches (rts::kQuerySlots, used in turn)
+  uint64_t query_next = 0;
   void *agg_dev = nullptr;    // compaction scratch (tile counts and offsets)
   size_t agg_bytes = 0;
   rts::BatchScratch *batch = nullptr;

@@ -233,19 +233,28 @@ __global__ void __launch_bounds__(kThreads) bitmap_count_kernel(const uint32_t *
   block_count(count, cnt);
 }
 
-__global__ void fill_range_kernel(uint32_t *out, uint64_t nrows, uint32_t ones) {
+// Every word of a bitmap set to all ones or all zeros (the tail bits past
+// nrows zero), 16-byte stores where the bitmap is aligned; the count, when
+// given, is stored by the first thread.
+__global__ void fill_range_kernel(uint32_t *out, uint64_t nrows, uint32_t ones, unsigned long long *count, int vec) {
   const uint64_t words = (nrows + 31) >> 5;
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint32_t rem = (uint32_t)(nrows & 31);
-  for (uint64_t i = tid; i < words; i += stride) {
-    uint32_t w = ones ? 0xFFFFFFFFu : 0u;
+  const uint32_t v = ones ? 0xFFFFFFFFu : 0u;
+  if (count && tid == 0) *count = ones ? (unsigned long long)nrows : 0ull;
+  uint64_t done = 0;
+  if (vec && words > 0) {
+    const uint64_t nv = (words - 1) / 4;  // vectors entirely before the last word
+    for (uint64_t i = tid; i < nv; i += stride) reinterpret_cast<uint4 *>(out)[i] = make_uint4(v, v, v, v);
+    done = nv * 4;
+  }
+  for (uint64_t i = done + tid; i < words; i += stride) {
+    uint32_t w = v;
     if (rem && i == words - 1) w &= ~(0xFFFFFFFFu >> rem);
     out[i] = w;
   }
 }
-
-__global__ void store_count_kernel(unsigned long long *count, unsigned long long v) { *count = v; }
 
 int grid_for(uint64_t items, int per_thread, int sm_count) {
   uint64_t threads = (items + per_thread - 1) / per_thread;
@@ -289,8 +298,7 @@ cudaError_t preload_separate_scan_kernels() {
                            reinterpret_cast<const void *>(scan_fused_kernel<0, false>),
                            reinterpret_cast<const void *>(bitmap_op_kernel),
                            reinterpret_cast<const void *>(bitmap_count_kernel),
-                           reinterpret_cast<const void *>(fill_range_kernel),
-                           reinterpret_cast<const void *>(store_count_kernel)};
+                           reinterpret_cast<const void *>(fill_range_kernel)};
   for (const void *k : kernels) {
     cudaFuncAttributes a;
     const cudaError_t e = cudaFuncGetAttributes(&a, k);
@@ -303,9 +311,9 @@ cudaError_t preload_separate_scan_kernels() {
 
 void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count, int sm_count,
                        cudaStream_t s) {
-  uint64_t words = (nrows + 31) >> 5;
-  if (words) fill_range_kernel<<<grid_for(words, 4, sm_count), kThreads, 0, s>>>(out, nrows, ones ? 1u : 0u);
-  if (count) store_count_kernel<<<1, 1, 0, s>>>(count, ones ? (unsigned long long)nrows : 0ull);
+  const uint64_t words = (nrows + 31) >> 5;
+  const bool vec = ((uintptr_t)out & 15) == 0;
+  fill_range_kernel<<<grid_for(words, 16, sm_count), kThreads, 0, s>>>(out, nrows, ones ? 1u : 0u, count, vec ? 1 : 0);
 }
 
 }  // namespace rts
