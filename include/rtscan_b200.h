@@ -267,7 +267,9 @@ typedef struct rts_batch_config {
                                    tested term by term, and passes of one query (or two or
                                    three with at most six terms) run as one fused scan per
                                    query; 3: 256-query passes, one 256-row block per warp */
-  int32_t warps_per_cta;        /* variant 3: 8 or 16 (each warp stages 8 KiB of result words) */
+  int32_t warps_per_cta;        /* 8 or 16.  Variant 4: CTA-wide blocks of 32 x 16 x warps / (slot
+                                   groups) rows, two 8-warp CTAs per SM when the pass's tables
+                                   leave room; variant 3: each warp stages 8 KiB of result words */
   int32_t max_queries_per_pass; /* 1..512 (variant 4), 1..256 (variant 3) */
   uint32_t table_budget_bytes;  /* shared memory a pass may use for its mask tables: 4 KiB up to
                                    136 KiB (variant 4), 88 KiB (variant 3, 16 warps), 140 KiB (8 warps) */

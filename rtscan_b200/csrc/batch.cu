@@ -17,7 +17,7 @@
 //     32 slots).  A row's verdict for all queries is the AND of its columns'
 //     table rows: C shared-memory loads per row and group of 32 queries
 //     instead of up to 2*C compares per row and query.
-//   * Variant 4 (default, batch4.cuh): CTA-wide blocks of 1024-4096 rows;
+//   * Variant 4 (default, batch4.cuh): CTA-wide blocks of 512-4096 rows;
 //     each lane ANDs the masks of 32 rows for one group, transposes the
 //     32x32 bit block in registers and stages the words for whole-line
 //     stores.  Passes of at most 20 queries skip the tables and test each
@@ -357,28 +357,53 @@ void launch_one(const BatchPass &bp, int sm_count, cudaStream_t s) {
 #include "batch4.cuh"
 #include "batch_few.cuh"
 
-template <int CMAX, int GV>
+template <int CMAX, int GV, int W>
 size_t smem_bytes4(uint32_t blob_words) {
-  return ((blob_words + 3) & ~3u) * 4 + (size_t)kV4StageWords * 4 + (size_t)kV4PosBytes<CMAX, GV>;
+  return ((blob_words + 3) & ~3u) * 4 + (size_t)V4Shape<GV, W>::kStage * 4 + (size_t)kV4PosBytes<CMAX, GV, W>;
 }
 
 // Shared memory of a variant-4 pass: `groups` slot groups over up to `cmax`
-// columns, blob of `blob_words` words.
-size_t pass_smem4(size_t blob_words, int cmax, int groups) {
+// columns, blob of `blob_words` words, CTAs of `warps` warps.
+size_t pass_smem4(size_t blob_words, int cmax, int groups, int warps) {
   const uint32_t w = (uint32_t)std::min<size_t>(blob_words, 1u << 30);
-  if (cmax <= 4) return groups == 4 ? smem_bytes4<4, 4>(w) : groups == 8 ? smem_bytes4<4, 8>(w) : smem_bytes4<4, 16>(w);
-  return groups == 4 ? smem_bytes4<8, 4>(w) : groups == 8 ? smem_bytes4<8, 8>(w) : smem_bytes4<8, 16>(w);
+  if (warps == 8) {
+    if (cmax <= 4)
+      return groups == 4 ? smem_bytes4<4, 4, 8>(w) : groups == 8 ? smem_bytes4<4, 8, 8>(w) : smem_bytes4<4, 16, 8>(w);
+    return groups == 4 ? smem_bytes4<8, 4, 8>(w) : groups == 8 ? smem_bytes4<8, 8, 8>(w) : smem_bytes4<8, 16, 8>(w);
+  }
+  if (cmax <= 4)
+    return groups == 4 ? smem_bytes4<4, 4, 16>(w) : groups == 8 ? smem_bytes4<4, 8, 16>(w) : smem_bytes4<4, 16, 16>(w);
+  return groups == 4 ? smem_bytes4<8, 4, 16>(w) : groups == 8 ? smem_bytes4<8, 8, 16>(w) : smem_bytes4<8, 16, 16>(w);
 }
 
-template <int CMAX, int GV>
+template <int CMAX, int GV, int W>
 void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
   static std::atomic<uint64_t> raised{0};
-  raise_smem_limit(batch4_kernel<CMAX, GV>, raised, 227 * 1024);
-  const size_t sm = smem_bytes4<CMAX, GV>(bp.blob_words);
+  raise_smem_limit(batch4_kernel<CMAX, GV, W>, raised, 227 * 1024);
+  const size_t sm = smem_bytes4<CMAX, GV, W>(bp.blob_words);
   if (sm > 227 * 1024) throw Error(RTS_ERR_ARG, "batch pass exceeds shared memory");
+  int per = 1;  // CTAs per SM: one, or two 8-warp CTAs when the shared memory holds both
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch4_kernel<CMAX, GV, W>, W * 32, sm) != cudaSuccess ||
+      per < 1) {
+    cudaGetLastError();
+    per = 1;
+  }
   const uint64_t want = bp.nblocks - bp.block_begin;
-  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count));
-  batch4_kernel<CMAX, GV><<<grid, kV4Threads, sm, s>>>(bp);
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count * per));
+  batch4_kernel<CMAX, GV, W><<<grid, W * 32, sm, s>>>(bp);
+}
+
+template <int CMAX, int W>
+void launch_shape4(const BatchPass &bp, int groups, int sm_count, cudaStream_t s) {
+  if (groups == 16) launch_one4<CMAX, 16, W>(bp, sm_count, s);
+  else if (groups == 8) launch_one4<CMAX, 8, W>(bp, sm_count, s);
+  else launch_one4<CMAX, 4, W>(bp, sm_count, s);
+}
+
+// Rows per block of a variant-4 pass shape.
+uint64_t rows_per_block4(int groups, int warps) {
+  const int tiles_per_warp = 32 / groups;
+  return (uint64_t)warps * tiles_per_warp * 32;
 }
 
 }  // namespace
@@ -538,6 +563,7 @@ struct BatchPlan {
     size_t off;  // word offset of the pass in `blob`
     int cmax;
     int variant;  // kernel the pass was planned for (3: 256-slot warps, 4: CTA-wide blocks)
+    int warps;    // variant 4: warps per CTA the pass was planned for (8 or 16)
     int groups;   // 32-slot groups of the pass (table words per position)
     bool few;     // at most kFewMaxQueries queries: tested term by term (batch_few_kernel), no tables
     FewPass fp;
@@ -560,7 +586,7 @@ int launch_outside(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::
     uint32_t *bm = out + o * stride_words;
     if (q.empty || q.cols.empty()) {
       launch_fill_range(bm, n, !q.empty, counts + o, ctx->sm_count, s);
-      launches += 2;
+      launches += 1;
       continue;
     }
     ScanParams sp;
@@ -648,6 +674,7 @@ int pass_groups(int nq) { return nq <= 128 ? 4 : nq <= 256 ? 8 : 16; }
 BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
                      const int32_t *out_index, size_t table_budget) {
   const int variant = ctx->batch_cfg.variant == 4 ? 4 : 3;
+  const int warps4 = ctx->batch_cfg.warps_per_cta == 8 ? 8 : 16;
   const int G = variant == 4 ? 16 : kGroups;  // pass capacity in groups (budgeted at this table width)
   std::vector<PassPlan> passes;
   for (int qi : which) {
@@ -669,6 +696,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
       FewPass &fp = b.fp;
       b.few = true;
       b.variant = variant;
+      b.warps = warps4;
       b.groups = 1;
       b.cmax = C <= 4 ? 4 : 8;
       fp.nq = (int)pp.qs.size();
@@ -756,7 +784,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     if (variant == 4) {
       size_t w = blob.size() + 32 * (size_t)Gp;  // tables so far, slot map
       for (int c = 0; c < C; c++) w += bp.m[c] + (bp.m[c] ? (buckets_for(bp.m[c], 16) + 3) / 2 : 1);
-      if (pass_smem4(w, C <= 4 ? 4 : 8, Gp) <= 227 * 1024) per = 16;
+      if (pass_smem4(w, C <= 4 ? 4 : 8, Gp, warps4) <= 227 * 1024) per = 16;
     }
     for (int c = 0; c < C; c++) {
       const uint32_t m = bp.m[c];
@@ -788,6 +816,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     for (int c = 0; c < C; c++) bp.col[c] = ctx->cols[pp.cols[c]];
     b.cmax = C <= 4 ? 4 : 8;
     b.variant = variant;
+    b.warps = warps4;
     while (plan.blob.size() % 4) plan.blob.push_back(0);  // 16-byte aligned pass start
     b.off = plan.blob.size();
     plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
@@ -875,10 +904,8 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
       launches++;
       continue;
     }
-    const uint64_t rows_per_block = b.variant != 4    ? (uint64_t)(32 * kTilesPerBlock)
-                                    : b.groups == 16 ? (uint64_t)V4Shape<16>::kRows
-                                    : b.groups == 8  ? (uint64_t)V4Shape<8>::kRows
-                                                     : (uint64_t)V4Shape<4>::kRows;
+    const uint64_t rows_per_block =
+        b.variant != 4 ? (uint64_t)(32 * kTilesPerBlock) : rows_per_block4(b.groups, b.warps);
     BatchPass bp = b.bp;
     bp.blob = dev_blob + b.off;
     bp.out = out;
@@ -893,13 +920,11 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
     if (b.variant == 4) {
       if (b.cmax == 4) {
-        if (b.groups == 16) launch_one4<4, 16>(bp, ctx->sm_count, s);
-        else if (b.groups == 8) launch_one4<4, 8>(bp, ctx->sm_count, s);
-        else launch_one4<4, 4>(bp, ctx->sm_count, s);
+        if (b.warps == 8) launch_shape4<4, 8>(bp, b.groups, ctx->sm_count, s);
+        else launch_shape4<4, 16>(bp, b.groups, ctx->sm_count, s);
       } else {
-        if (b.groups == 16) launch_one4<8, 16>(bp, ctx->sm_count, s);
-        else if (b.groups == 8) launch_one4<8, 8>(bp, ctx->sm_count, s);
-        else launch_one4<8, 4>(bp, ctx->sm_count, s);
+        if (b.warps == 8) launch_shape4<8, 8>(bp, b.groups, ctx->sm_count, s);
+        else launch_shape4<8, 16>(bp, b.groups, ctx->sm_count, s);
       }
     } else if (b.cmax == 4) {
       if (w8) launch_one<4, 8>(bp, ctx->sm_count, s);
@@ -1058,23 +1083,30 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     ctx->cols.clear();
     for (int c = 0; c < ncols; c++) ctx->cols.push_back(H.cols + cstride * c);
     ctx->nrows = nrows;
+    // On every way out: no copy from the caller's buffers is left in flight,
+    // and the context's own columns are back.
     struct Restore {
       rts_ctx *c;
       std::vector<const uint32_t *> cols;
       uint64_t n;
+      rts::HostBatchBuffers *h;
       ~Restore() {
+        cudaStreamSynchronize(h->up);
+        cudaStreamSynchronize(h->compute);
+        cudaStreamSynchronize(h->copy);
         c->cols = cols;
         c->nrows = n;
       }
-    } restore{ctx, saved_cols, saved_n};
+    } restore{ctx, saved_cols, saved_n, &H};
     // Row-chunked pipeline over three streams: the upload of chunk r+1 and
     // the download of chunk r-1's words of every bitmap (one 2D copy) run
     // while chunk r is scanned, so the column upload hides under the bitmap
     // download.  Chunks are multiples of 4096 rows (the largest kernel block).
-    std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms, offsets, nq);
-    std::vector<int> inside, outside;
-    for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
-    const uint64_t want_chunks = std::max<uint64_t>(1, std::min<uint64_t>(8, nrows >> 22));
+    // Chunks of about 2^22 rows (at most 32): the first download starts
+    // after one chunk's upload and scan.  Each chunk's upload is queued with
+    // its scan (queueing every upload first measured 21 ms slower per 1e8 x 4
+    // call: the downloads then share the link with 1.6 GB of uploads).
+    const uint64_t want_chunks = std::max<uint64_t>(1, std::min<uint64_t>(32, nrows >> 22));
     const uint64_t chunk_rows = ((nrows + want_chunks - 1) / want_chunks + 4095) / 4096 * 4096;
     const int nchunks = (int)((nrows + chunk_rows - 1) / chunk_rows);
     while ((int)H.ev.size() < 2 * nchunks + 1) {
@@ -1082,6 +1114,9 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       RTS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       H.ev.push_back(e);
     }
+    std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms, offsets, nq);
+    std::vector<int> inside, outside;
+    for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
     if (nq > 0) RTS_CUDA(cudaMemsetAsync(H.counts, 0, (size_t)nq * 8, H.compute));
     rts::BatchPlan plan;
     const uint32_t *dev_blob = nullptr;

@@ -4,9 +4,10 @@
 //
 // A pass has GV groups of 32 query slots (GV = 16, 8 or 4: 512, 256 or 128
 // slots; the planner picks the smallest that holds the pass), and its
-// tables hold GV words per interval position.  A CTA of 16 warps works on
-// blocks of 32 x 512 / GV rows (1024, 2048, 4096): tiles of 32 rows, 32 / GV
-// tiles per warp, and all slots of the pass at once:
+// tables hold GV words per interval position.  A CTA of W warps (16, or 8
+// so that two CTAs can share an SM when the tables are small) works on
+// blocks of W x 32 x 32 / GV rows (1024, 2048, 4096 for 16 warps): tiles of
+// 32 rows, 32 / GV tiles per warp, and all slots of the pass at once:
 //   1. every thread finds the interval positions of 32 / GV rows (one per
 //      column) and writes their table word offsets to shared memory, while
 //      the previous block's result words are stored;
@@ -17,28 +18,32 @@
 //      and writes the 32 words to a shared-memory stage laid out
 //      [query][tiles of the block] with word index t ^ ((32 / GV) * g),
 //      which puts the 32 lanes of a warp in 32 different banks;
-//   3. each warp stores 2 * GV queries' rows of the stage: a query's words
-//      for the block (128 bytes per 1024 rows) leave as 16-byte stores from
-//      128 / GV lanes, whole 128-byte lines.
+//   3. each warp stores 32 * GV / W queries' rows of the stage: a query's
+//      words for the block (128 bytes per 1024 rows) leave as 16-byte stores
+//      from 128 / GV lanes, whole 128-byte lines.
 // No cross-lane exchange is needed, and positions are shared by all queries
 // of the pass.  For 512- and 256-slot passes over up to 4 columns, step 1
 // for the next block runs inside step 2 (see the kernel).
-constexpr int kV4Warps = 16;
-constexpr int kV4Threads = kV4Warps * 32;
-constexpr int kV4StageWords = 16384;  // 64 KB: slots x words per query per block, for every GV
-constexpr int kV4MaxRows = 4096;      // rows per block of the smallest pass shape
-
-template <int GV>
+template <int GV, int W>
 struct V4Shape {
   static_assert(GV == 16 || GV == 8 || GV == 4, "512-, 256- or 128-slot passes");
+  static_assert(W == 16 || W == 8, "8 or 16 warps per CTA");
+  static constexpr int kThreads = W * 32;
   static constexpr int kTPW = 32 / GV;               // tiles per warp
-  static constexpr int kTiles = kV4Warps * kTPW;     // tiles per block = words per query per block
+  static constexpr int kTiles = W * kTPW;            // tiles per block = words per query per block
   static constexpr int kRows = kTiles * 32;          // rows per block
   static constexpr int kSlots = 32 * GV;
-  static constexpr int kRPT = kRows / kV4Threads;    // rows per thread in step 1
-  static constexpr int kLPQ = 128 / GV;              // lanes per query row in step 3 (16-byte chunks)
+  static constexpr int kStage = kSlots * kTiles;     // stage words: 1024 * W
+  static constexpr int kRPT = kRows / kThreads;      // rows per thread in step 1
+  static constexpr int kLPQ = kTiles / 4;            // lanes per query row in step 3 (16-byte chunks)
   static constexpr int kQPI = 32 / kLPQ;             // queries per store instruction
-  static_assert(kSlots * kTiles == kV4StageWords, "stage size");
+  static constexpr int kQPW = kSlots / W;            // queries each warp stores in step 3
+  static constexpr int kIters = kQPW / kQPI;         // store instructions per warp and block (8)
+  // Stage word-index XOR of group g: kTPW * g, kept below kTiles (with 16
+  // warps it always is; 512 slots on 8 warps fold it, and their stage
+  // writes then meet two to a bank)
+  static __device__ __forceinline__ int swizzle(int g) { return (kTPW * g) & (kTiles - 1); }
+  static_assert(kIters == 8, "eight store instructions per warp");
 };
 
 // Per row and column the position buffer holds the word offset of the row's
@@ -47,8 +52,9 @@ struct V4Shape {
 // under 2^16 words), one padding row per tile.
 template <int CMAX>
 using V4Pos = typename std::conditional<(CMAX <= 4), uint32_t, uint16_t>::type;
-template <int CMAX, int GV>
-constexpr int kV4PosBytes = (V4Shape<GV>::kRows + V4Shape<GV>::kTiles) * CMAX * (int)sizeof(V4Pos<CMAX>);
+template <int CMAX, int GV, int W>
+constexpr int kV4PosBytes =
+    (V4Shape<GV, W>::kRows + V4Shape<GV, W>::kTiles) * CMAX * (int)sizeof(V4Pos<CMAX>);
 
 // Exchange the bits of a under mask M << S with the bits of b under M (a
 // delta swap: the XOR of the two bit sets applied to both; measured faster
@@ -95,13 +101,14 @@ __device__ __forceinline__ void transpose32(uint32_t (&x)[32]) {
   }
 }
 
-template <int CMAX, int GV>
-__global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_constant__ BatchPass p) {
-  using S = V4Shape<GV>;
+template <int CMAX, int GV, int W>
+__global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_constant__ BatchPass p) {
+  using S = V4Shape<GV, W>;
+  constexpr int kV4Threads = S::kThreads;
   extern __shared__ __align__(16) uint32_t smem[];
   uint32_t *blob = smem;
   uint32_t *stage = smem + ((p.blob_words + 3) & ~3u);
-  V4Pos<CMAX> *posbuf = reinterpret_cast<V4Pos<CMAX> *>(stage + kV4StageWords);
+  V4Pos<CMAX> *posbuf = reinterpret_cast<V4Pos<CMAX> *>(stage + S::kStage);
 
   for (uint32_t i = threadIdx.x; i < p.blob_words; i += blockDim.x) blob[i] = __ldg(p.blob + i);
   __syncthreads();
@@ -111,14 +118,13 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
   const int32_t *slot_query = reinterpret_cast<const int32_t *>(blob + p.slot_off);
   // step-2 identity
   const int tile = S::kTPW * warp + lane / GV, g = lane % GV;
-  // step-3 identity: queries warp * 2GV + it * kQPI + qq, 16-byte chunk `chunk` of their row
+  // step-3 identity: queries warp * kQPW + it * kQPI + qq, 16-byte chunk
+  // `chunk` of their row; the stage word-index XOR of query q's group is
+  // kTPW * (q / 32), constant over the kQPI queries of one instruction
   const int qq = lane / S::kLPQ, chunk = lane % S::kLPQ;
-  const int sw = S::kTPW * (warp * GV / 16);  // stage word-index XOR of this warp's queries
-  const int pchunk = chunk ^ (sw >> 2);       // physical chunk of logical chunk `chunk`
-  const bool swap_pairs = sw & 2;             // words k and k^2 swapped inside a chunk
-  uint32_t cnt[8];
+  uint32_t cnt[S::kIters];
 #pragma unroll
-  for (int i = 0; i < 8; i++) cnt[i] = 0;
+  for (int i = 0; i < S::kIters; i++) cnt[i] = 0;
 
   // For 512- and 256-slot passes over up to 4 columns (3-5 % faster for the
   // 256-slot shape, 4-10 % slower for the 128-slot one, whose 8 rows per
@@ -249,11 +255,13 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
       const uint64_t word0 = prev * S::kTiles;
       const bool full = p.vec_store && word0 + S::kTiles <= p.words;
 #pragma unroll
-      for (int it = 0; it < 8; it++) {
-        const int q = warp * 2 * GV + it * S::kQPI + qq;
+      for (int it = 0; it < S::kIters; it++) {
+        const int q = warp * S::kQPW + it * S::kQPI + qq;
+        const int sw = S::swizzle((warp * S::kQPW + it * S::kQPI) >> 5);
+        const int pchunk = chunk ^ (sw >> 2);  // physical chunk of logical chunk `chunk`
         const int32_t sq = slot_query[q];
         uint4 v = *reinterpret_cast<const uint4 *>(stage + q * S::kTiles + pchunk * 4);
-        if (swap_pairs) v = make_uint4(v.z, v.w, v.x, v.y);
+        if (sw & 2) v = make_uint4(v.z, v.w, v.x, v.y);  // words k and k^2 swapped inside a chunk
         cnt[it] += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
         if (sq >= 0) {
           uint32_t *dst = p.out + (uint64_t)sq * p.stride_words + word0 + chunk * 4;
@@ -326,7 +334,7 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
 #pragma unroll
         for (int j = 0; j < 32; j++) acc[j] &= vm;
       }
-      const int col = tile ^ (S::kTPW * g);
+      const int col = tile ^ S::swizzle(g);
 #pragma unroll
       for (int j = 0; j < 32; j++) stage[(32 * g + j) * S::kTiles + col] = acc[j];
     }
@@ -337,11 +345,11 @@ __global__ void __launch_bounds__(kV4Threads, 1) batch4_kernel(const __grid_cons
   }
   // counts: the kLPQ lanes of a query row hold partial counts of that query
 #pragma unroll
-  for (int it = 0; it < 8; it++) {
+  for (int it = 0; it < S::kIters; it++) {
     uint32_t c = cnt[it];
 #pragma unroll
     for (int o = 1; o < S::kLPQ; o <<= 1) c += __shfl_xor_sync(kFull, c, o);
-    const int q = warp * 2 * GV + it * S::kQPI + qq;
+    const int q = warp * S::kQPW + it * S::kQPI + qq;
     const int32_t sq = slot_query[q];
     if (chunk == 0 && sq >= 0 && c) atomicAdd(p.counts + sq, (unsigned long long)c);
   }

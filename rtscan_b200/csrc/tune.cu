@@ -9,8 +9,9 @@
 // queries, keeps the fastest, and can cache the choice in a small text file
 // keyed by GPU, SM count, column count, table size and batch size.
 //
-// Candidates: variant 4 (one 16-warp CTA per SM, pass shapes of 128/256/512
-// slots) at seven pass sizes from 128 to 512 queries and two table budgets,
+// Candidates: variant 4 (pass shapes of 128/256/512 slots) with 16-warp
+// CTAs at seven pass sizes from 128 to 512 queries and two table budgets,
+// and with 8-warp CTAs (one per SM, or two when small tables leave room),
 // and variant 3 at 8 and 16 warps per CTA with two budgets each.  The sample
 // is the table's first rows: as many as the result bitmaps of the batch fit
 // in a quarter of the free device memory, at least 2^24 and at most 2^27
@@ -38,6 +39,10 @@ std::vector<Candidate> candidates() {
   std::vector<Candidate> c;
   for (int qpp : {512, 448, 384, 320, 256, 192, 128})
     for (size_t budget : {(size_t)136 * 1024, (size_t)112 * 1024}) c.push_back({4, 16, qpp, budget});
+  // 8-warp CTAs: one per SM with large tables, or two per SM when the
+  // tables stay under about 56 KiB
+  for (int qpp : {512, 256}) c.push_back({4, 8, qpp, (size_t)136 * 1024});
+  for (int qpp : {512, 256, 128}) c.push_back({4, 8, qpp, (size_t)56 * 1024});
   for (size_t budget : {(size_t)88 * 1024, (size_t)64 * 1024}) c.push_back({3, 16, 256, budget});
   for (size_t budget : {(size_t)140 * 1024, (size_t)40 * 1024}) c.push_back({3, 8, 256, budget});
   return c;

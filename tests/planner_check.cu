@@ -59,8 +59,9 @@ void check_table_pass(const rts::BatchPlan &plan, const rts::BatchPlan::Pass &b,
   CHECK(G == 4 || G == 8 || G == 16, "table pass with %d groups", G);
   CHECK(nq > rts::kFewMaxQueries, "table pass of %d queries", nq);
   CHECK(rts::pass_groups(nq) == G, "%d queries in a %d-group pass", nq, G);
-  CHECK(rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G) <= 227 * 1024, "pass needs %zu bytes of shared memory",
-        rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G));
+  CHECK(b.warps == 8 || b.warps == 16, "pass planned for %d warps", b.warps);
+  CHECK(rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G, b.warps) <= 227 * 1024,
+        "pass needs %zu bytes of shared memory", rts::pass_smem4(bp.blob_words, bp.ncols <= 4 ? 4 : 8, G, b.warps));
   for (int s = 0; s < 32 * G; s++)
     if (slot[s] >= 0) {
       CHECK(slot[s] < (int)seen.size(), "slot maps to query %d", slot[s]);
@@ -152,6 +153,7 @@ int main(int argc, char **argv) {
     ctx->sm_count = 148;
     const size_t budgets[] = {136 * 1024, 64 * 1024, 8 * 1024};
     ctx->batch_cfg.table_budget = budgets[rng() % 3];
+    ctx->batch_cfg.warps_per_cta = rng() % 2 ? 16 : 8;  // 8-warp passes fit more blob beside a smaller stage
     const int nq = rng() % 4 ? counts[rng() % (sizeof counts / sizeof counts[0])] : 1 + (int)(rng() % 1100);
     // bounds from a small pool (shared boundaries, domain edges) and random values
     std::vector<uint32_t> pool = {0, 1, 2, kMax - 1, kMax, 1u << 31};

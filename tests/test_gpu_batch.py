@@ -182,6 +182,8 @@ def test_batch_alone_and_in_the_mix(ctx):
 
 
 @pytest.mark.parametrize("cfg", [(4, 16, 512, 136 * 1024), (4, 16, 100, 136 * 1024), (4, 16, 512, 8 * 1024),
+                                 (4, 8, 512, 136 * 1024), (4, 8, 512, 56 * 1024), (4, 8, 256, 56 * 1024),
+                                 (4, 8, 128, 56 * 1024), (4, 8, 100, 136 * 1024),
                                  (3, 16, 256, 88 * 1024), (3, 16, 64, 16 * 1024), (3, 8, 256, 40 * 1024),
                                  (3, 8, 128, 140 * 1024), (3, 8, 1, 4096), (4, 16, 1, 4096)])
 def test_batch_every_launch_shape(ctx, cfg):
@@ -284,6 +286,25 @@ def test_batch_host_buffers(ctx, n, nq):
         want, wcnt = expect(cols, q)
         assert int(counts[i]) == wcnt, (i, q)
         assert np.array_equal(bms[i, :R.bitmap_words(n)], want), (i, q)
+    assert ctx.nrows == 1000
+
+
+def test_batch_host_buffers_many_chunks_and_a_refused_query(ctx):
+    """A table of four row chunks: every upload is queued before the batch is
+    planned, and a batch the planner refuses (a term on a column the call
+    does not pass) fails with RTS_ERR_ARG after those uploads have finished,
+    leaving the context usable for the next call."""
+    n = (1 << 24) + 12_345
+    ctx.load_columns([D.uniform(1000, 1)])
+    cols = [D.uniform(n, 600), D.zipf(n, 601, 1.1), D.normal(n, 602)]
+    qs = D.batch_queries(cols, 300, seed=18)
+    with pytest.raises(R.RtsError) as e:
+        ctx.scan_batch_host(cols, qs + [[(5, 0, 9)]])
+    assert e.value.code == -1
+    bms, counts = ctx.scan_batch_host(cols, qs)
+    for i in (0, 1, 150, 299):
+        want, wcnt = expect(cols, qs[i])
+        assert int(counts[i]) == wcnt and np.array_equal(bms[i, :R.bitmap_words(n)], want), i
     assert ctx.nrows == 1000
 
 

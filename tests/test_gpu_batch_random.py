@@ -3,7 +3,8 @@
 pass routing: one to three queries (fused scans per query when narrow), up
 to 20 (term by term), 21-128, 129-256 and 257-512 (the 128-, 256- and
 512-slot tables), more than 512 (several passes).  Queries over up to 8
-columns, plus empty and unconstrained ones.  Every bitmap and count must
+columns, plus empty and unconstrained ones.  Odd trials run the table
+passes on 8-warp CTAs (one or two per SM).  Every bitmap and count must
 equal the scalar filter's."""
 import numpy as np
 import pytest
@@ -52,8 +53,15 @@ def test_random_batch(ctx, trial):
     stride = words + (trial % 5)
     out = torch.full((len(qs) * stride,), -1, dtype=torch.int32, device="cuda")
     cnt = torch.full((len(qs),), -1, dtype=torch.int64, device="cuda")
-    ctx.scan_batch_async(qs, out.data_ptr(), stride, cnt.data_ptr(), torch.cuda.current_stream().cuda_stream)
-    torch.cuda.synchronize()
+    old = ctx.batch_config()
+    if trial % 2:  # odd trials: 8-warp CTAs for the table passes
+        ctx.set_batch_config(4, 8, 512, 136 * 1024 if trial % 4 == 1 else 56 * 1024)
+    try:
+        ctx.scan_batch_async(qs, out.data_ptr(), stride, cnt.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_batch_config(old["variant"], old["warps_per_cta"], old["max_queries_per_pass"],
+                             old["table_budget_bytes"])
     o = out.cpu().numpy().view(np.uint32)
     c = cnt.cpu().numpy()
     for i, q in enumerate(qs):
