@@ -80,3 +80,29 @@ def test_bench_help_runs_without_a_gpu():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0 and "--impl" in r.stdout
+
+
+def test_every_scan_configuration_is_in_the_line(line):
+    """The plain single-column 1e8-row scan (>= 70 % of the HBM peak), the
+    2-4 column conjunctions fused and separate, the selectivity sweep on
+    uniform, 256- and 64-value columns through the fused scan and the BinDex,
+    and the served rates 1k-50k q/s with the highest rate kept up with."""
+    s = line["single_1e8"]
+    assert s["frac"] >= 0.70 and abs(s["frac"] - s["GB_s"] / s["peak"]) < 0.002
+    m = line["multi_1e8"]["queries"]
+    assert [q["columns"] for q in m] == [2, 3, 4] and all(q["equal"] for q in m)
+    sw = line["sweep_1e8"]["queries"]
+    assert {q["column"] for q in sw} == {"uniform", "range:0:256", "range:0:64"}
+    assert {q["target"] for q in sw if q["column"] == "uniform"} == {0.001, 0.01, 0.1, 0.5, 0.9}
+    assert all(q["equal"] for q in sw)
+    rates = [r["offered_qps"] for r in line["served"]["rates"]]
+    assert min(rates) <= 1000 and max(rates) >= 50000
+    top = line["served"]["max_sustained"]
+    assert top["offered_qps"] in rates and top["achieved_qps"] >= 0.98 * top["offered_qps"]
+
+
+def test_autotune_report_in_the_line(line):
+    a = line["batch_config"]["autotune"]
+    assert a["sample_rows"] == line["config"]["nrows_per_gpu"] and len(a["candidates"]) >= 18
+    assert {c["warps_per_cta"] for c in a["candidates"]} == {8, 16}
+    assert a["best_ms"] == min(c["ms"] for c in a["candidates"])
