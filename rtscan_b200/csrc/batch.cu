@@ -73,6 +73,8 @@ struct BatchPass {
   uint64_t nblocks;             // end of the range, in blocks
   int vec_store;                // bitmaps 16-byte aligned (out and stride)
   uint32_t word_bytes;          // 4, passed at run time (see the mask loop of batch4_kernel)
+  const uint2 *pre;             // shared positions: the pass's table word offsets of row r at pre[r - pre_row0]
+  uint64_t pre_row0;
 };
 
 // Log-linear bucket of v >= 0 with M mantissa bits: v itself below 2^M,
@@ -126,6 +128,75 @@ __device__ __forceinline__ uint32_t position(const BatchPass &p, const uint32_t 
     if (B[mid] <= x) lo = mid + 1; else hi = mid;
   }
   return lo;
+}
+
+// Shared positions.  A batch of several table passes searches every row's
+// position once per column, among the union of the passes' boundaries
+// (each pass's boundaries are a subset of the union, so a union position
+// fixes the position in every pass), and maps it through one small table
+// per pass and column to that pass's table word offset.  The passes then
+// read four 16-bit offsets per row instead of searching (batch4_kernel with
+// PRE).
+constexpr int kMaxPrePasses = 4;
+
+struct PreParams {
+  BatchPass u;                         // the union columns: col, m, bmin, bmax, shift, lgm, bnd_off, bkt_off,
+                                       // nbk, ncols, blob, blob_words
+  uint32_t lut_off[kMaxPrePasses][4];  // pass p, its column c: first entry (in 16-bit units of the blob) of the
+                                       // union position -> table word offset map (m + 1 entries)
+  int32_t ucol[kMaxPrePasses][4];      // union column of pass p's column c (-1: the pass has no column c)
+  int npass;
+  uint64_t row_begin, row_end;
+  uint2 *out;                          // out[p * stride + (row - row_begin)]: four offsets, two per word
+  uint64_t stride;
+};
+
+__device__ __forceinline__ uint32_t pick4(const uint32_t (&v)[4], int i) {
+  return i == 0 ? v[0] : i == 1 ? v[1] : i == 2 ? v[2] : v[3];
+}
+
+constexpr int kPreThreads = 512;
+constexpr int kPreRows = 4;  // rows per thread and iteration: their loads and searches overlap
+
+__global__ void __launch_bounds__(kPreThreads) pre_kernel(const __grid_constant__ PreParams P) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  for (uint32_t i = threadIdx.x; i < P.u.blob_words; i += blockDim.x) smem[i] = __ldg(P.u.blob + i);
+  __syncthreads();
+  const uint16_t *lut = reinterpret_cast<const uint16_t *>(smem);
+  const uint64_t tile = (uint64_t)kPreThreads * kPreRows;  // rows of one block iteration
+  for (uint64_t base = P.row_begin + (uint64_t)blockIdx.x * tile; base < P.row_end; base += (uint64_t)gridDim.x * tile) {
+    uint32_t x[kPreRows][4];
+#pragma unroll
+    for (int r = 0; r < kPreRows; r++) {
+      const uint64_t row = base + threadIdx.x + (uint64_t)r * kPreThreads;
+#pragma unroll
+      for (int u = 0; u < 4; u++) x[r][u] = (u < P.u.ncols && row < P.row_end) ? __ldg(P.u.col[u] + row) : 0u;
+    }
+    // the searches of the thread's rows and columns are independent, so
+    // their shared-memory loads overlap (a loop-free lookup with a fallback
+    // search, or eight rows per thread, measured slower)
+    uint32_t pos[kPreRows][4];
+#pragma unroll
+    for (int r = 0; r < kPreRows; r++)
+#pragma unroll
+      for (int u = 0; u < 4; u++) pos[r][u] = u < P.u.ncols ? position(P.u, smem, u, x[r][u]) : 0u;
+#pragma unroll
+    for (int r = 0; r < kPreRows; r++) {
+      const uint64_t row = base + threadIdx.x + (uint64_t)r * kPreThreads;
+      if (row >= P.row_end) continue;
+#pragma unroll
+      for (int q = 0; q < kMaxPrePasses; q++) {
+        if (q >= P.npass) break;
+        uint32_t o[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const int u = P.ucol[q][c];
+          o[c] = u >= 0 ? lut[P.lut_off[q][c] + pick4(pos[r], u)] : 0u;
+        }
+        P.out[q * P.stride + (row - P.row_begin)] = make_uint2(o[0] | (o[1] << 16), o[2] | (o[3] << 16));
+      }
+    }
+  }
 }
 
 // 8x8 bit transposes in each byte lane of eight registers: on return, bit r
@@ -376,28 +447,40 @@ size_t pass_smem4(size_t blob_words, int cmax, int groups, int warps) {
   return groups == 4 ? smem_bytes4<8, 4, 16>(w) : groups == 8 ? smem_bytes4<8, 8, 16>(w) : smem_bytes4<8, 16, 16>(w);
 }
 
-template <int CMAX, int GV, int W>
+template <int CMAX, int GV, int W, bool PRE>
 void launch_one4(const BatchPass &bp, int sm_count, cudaStream_t s) {
   static std::atomic<uint64_t> raised{0};
-  raise_smem_limit(batch4_kernel<CMAX, GV, W>, raised, 227 * 1024);
+  raise_smem_limit(batch4_kernel<CMAX, GV, W, PRE>, raised, 227 * 1024);
   const size_t sm = smem_bytes4<CMAX, GV, W>(bp.blob_words);
   if (sm > 227 * 1024) throw Error(RTS_ERR_ARG, "batch pass exceeds shared memory");
   int per = 1;  // CTAs per SM: one, or two 8-warp CTAs when the shared memory holds both
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch4_kernel<CMAX, GV, W>, W * 32, sm) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, batch4_kernel<CMAX, GV, W, PRE>, W * 32, sm) !=
+          cudaSuccess ||
       per < 1) {
     cudaGetLastError();
     per = 1;
   }
   const uint64_t want = bp.nblocks - bp.block_begin;
   const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count * per));
-  batch4_kernel<CMAX, GV, W><<<grid, W * 32, sm, s>>>(bp);
+  batch4_kernel<CMAX, GV, W, PRE><<<grid, W * 32, sm, s>>>(bp);
 }
 
 template <int CMAX, int W>
 void launch_shape4(const BatchPass &bp, int groups, int sm_count, cudaStream_t s) {
-  if (groups == 16) launch_one4<CMAX, 16, W>(bp, sm_count, s);
-  else if (groups == 8) launch_one4<CMAX, 8, W>(bp, sm_count, s);
-  else launch_one4<CMAX, 4, W>(bp, sm_count, s);
+  if (groups == 16) launch_one4<CMAX, 16, W, false>(bp, sm_count, s);
+  else if (groups == 8) launch_one4<CMAX, 8, W, false>(bp, sm_count, s);
+  else launch_one4<CMAX, 4, W, false>(bp, sm_count, s);
+}
+
+// A pass fed by shared positions (256 or 512 slots, four columns or fewer).
+void launch_pre4(const BatchPass &bp, int groups, int warps, int sm_count, cudaStream_t s) {
+  if (warps == 8) {
+    if (groups == 16) launch_one4<4, 16, 8, true>(bp, sm_count, s);
+    else launch_one4<4, 8, 8, true>(bp, sm_count, s);
+  } else {
+    if (groups == 16) launch_one4<4, 16, 16, true>(bp, sm_count, s);
+    else launch_one4<4, 8, 16, true>(bp, sm_count, s);
+  }
 }
 
 // Rows per block of a variant-4 pass shape.
@@ -543,7 +626,16 @@ struct BatchScratch {
     cudaEvent_t done = nullptr;
   } slot[2];
   int next = 0;
+  // shared positions of the context's batch calls: one buffer, and the
+  // event after the last launch that reads it (a call on another stream
+  // waits for it on the device)
+  void *pre = nullptr;
+  size_t pre_cap = 0;
+  cudaEvent_t pre_done = nullptr;
   ~BatchScratch() {
+    if (pre_done) cudaEventSynchronize(pre_done);
+    if (pre) cudaFree(pre);
+    if (pre_done) cudaEventDestroy(pre_done);
     for (auto &s : slot) {
       if (s.done) cudaEventSynchronize(s.done);
       if (s.dev) cudaFree(s.dev);
@@ -567,9 +659,13 @@ struct BatchPlan {
     int groups;   // 32-slot groups of the pass (table words per position)
     bool few;     // at most kFewMaxQueries queries: tested term by term (batch_few_kernel), no tables
     FewPass fp;
+    int pre_slot = -1;  // shared positions: this pass's slot in the scratch, or -1 (it searches)
   };
   std::vector<Pass> passes;
   std::vector<uint32_t> blob;
+  // shared positions of the passes with a pre_slot (npass 0: none)
+  PreParams pre;
+  size_t pre_off = 0;  // word offset of the union boundaries, buckets and maps in `blob`
 };
 
 // Answer the queries that do not run in the batch kernel (empty, no
@@ -669,10 +765,119 @@ bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && 
 // Slot groups of a variant-4 pass of nq queries.
 int pass_groups(int nq) { return nq <= 128 ? 4 : nq <= 256 ? 8 : 16; }
 
+// Shared positions for a plan with at least two table passes of the
+// look-ahead shapes (256 or 512 slots) over four columns or fewer whose
+// columns together are at most four: the union of their boundaries per
+// column with its bucket index, and per pass and column the map from a
+// union position to the pass's table word offset (a pass's boundaries are
+// a subset of the union, so the pass position of union position k is the
+// number of its boundaries <= B_u[k-1]).  Appended to the plan blob; other
+// plans are left as they are.
+void plan_shared_positions(BatchPlan &plan) {
+  plan.pre.npass = 0;
+  std::vector<int> which;
+  for (size_t i = 0; i < plan.passes.size(); i++) {
+    const BatchPlan::Pass &b = plan.passes[i];
+    if (!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 8 && (int)which.size() < kMaxPrePasses)
+      which.push_back((int)i);
+  }
+  if (which.size() < 2) return;
+  std::vector<const uint32_t *> ucols;
+  for (int i : which) {
+    const BatchPass &bp = plan.passes[i].bp;
+    for (int c = 0; c < bp.ncols; c++)
+      if (std::find(ucols.begin(), ucols.end(), bp.col[c]) == ucols.end()) ucols.push_back(bp.col[c]);
+  }
+  if (ucols.size() > 4) return;
+  const int U = (int)ucols.size();
+  std::vector<std::vector<uint32_t>> Bu(U);
+  for (int i : which) {
+    const BatchPlan::Pass &b = plan.passes[i];
+    const uint32_t *blob = plan.blob.data() + b.off;
+    for (int c = 0; c < b.bp.ncols; c++) {
+      const int u = (int)(std::find(ucols.begin(), ucols.end(), b.bp.col[c]) - ucols.begin());
+      Bu[u].insert(Bu[u].end(), blob + b.bp.bnd_off[c], blob + b.bp.bnd_off[c] + b.bp.m[c]);
+    }
+  }
+  for (auto &B : Bu) {
+    std::sort(B.begin(), B.end());
+    B.erase(std::unique(B.begin(), B.end()), B.end());
+    if (B.size() > 0xFFFEu) return;  // positions are 16-bit
+  }
+  PreParams &P = plan.pre;
+  memset(&P, 0, sizeof P);
+  std::vector<uint32_t> blob;  // boundaries | buckets | maps, offsets relative to its own start
+  BatchPass &u = P.u;
+  u.ncols = U;
+  for (int c = 0; c < U; c++) {
+    u.col[c] = ucols[c];
+    const uint32_t m = (uint32_t)Bu[c].size();
+    u.m[c] = m;
+    u.bnd_off[c] = (uint32_t)blob.size();
+    blob.insert(blob.end(), Bu[c].begin(), Bu[c].end());
+    if (m == 0) {
+      u.bkt_off[c] = (uint32_t)blob.size();
+      u.nbk[c] = 1;
+      blob.push_back(0);
+      continue;
+    }
+    u.bmin[c] = Bu[c].front();
+    u.bmax[c] = Bu[c].back();
+    uint32_t nb = 1;
+    while (nb < 16 * m && nb < 4096) nb <<= 1;
+    const uint64_t span = (uint64_t)u.bmax[c] - u.bmin[c] + 1;
+    const std::vector<uint16_t> bk = bucket_index(Bu[c], span, nb, &u.shift[c], &u.lgm[c]);
+    u.nbk[c] = (uint32_t)bk.size() - 1;
+    u.bkt_off[c] = (uint32_t)blob.size();
+    blob.resize(blob.size() + (bk.size() + 1) / 2, 0u);
+    memcpy(blob.data() + u.bkt_off[c], bk.data(), bk.size() * 2);
+  }
+  std::vector<uint16_t> maps;  // appended after the words above
+  for (int q = 0; q < (int)which.size(); q++) {
+    BatchPlan::Pass &b = plan.passes[which[q]];
+    const uint32_t *pblob = plan.blob.data() + b.off;
+    for (int c = 0; c < 4; c++) {
+      P.ucol[q][c] = -1;
+      if (c >= b.bp.ncols) continue;
+      const int uc = (int)(std::find(ucols.begin(), ucols.end(), b.bp.col[c]) - ucols.begin());
+      P.ucol[q][c] = uc;
+      P.lut_off[q][c] = (uint32_t)(blob.size() * 2 + maps.size());
+      const uint32_t *Bp = pblob + b.bp.bnd_off[c];
+      const uint32_t mp = b.bp.m[c];
+      const std::vector<uint32_t> &B = Bu[uc];
+      uint32_t j = 0;
+      for (size_t k = 0; k <= B.size(); k++) {
+        if (k > 0)
+          while (j < mp && Bp[j] <= B[k - 1]) j++;
+        const uint64_t off = (uint64_t)b.bp.tab_off[c] + (uint64_t)j * b.groups;
+        if (off > 0xFFFFu) {  // table offsets are 16-bit in the maps
+          plan.pre.npass = 0;
+          return;
+        }
+        maps.push_back((uint16_t)off);
+      }
+    }
+  }
+  if (maps.size() & 1) maps.push_back(0);
+  const size_t words = blob.size();
+  blob.resize(words + maps.size() / 2);
+  memcpy(blob.data() + words, maps.data(), maps.size() * 2);
+  if (blob.size() * 4 > 200 * 1024) {  // the pre kernel's shared memory
+    plan.pre.npass = 0;
+    return;
+  }
+  u.blob_words = (uint32_t)blob.size();
+  P.npass = (int)which.size();
+  for (int q = 0; q < P.npass; q++) plan.passes[which[q]].pre_slot = q;
+  while (plan.blob.size() % 4) plan.blob.push_back(0);
+  plan.pre_off = plan.blob.size();
+  plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
+}
+
 // Passes for the kernel queries `which` (indices into norm); query qi writes
 // bitmap out_index[qi] (qi when null).
 BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
-                     const int32_t *out_index, size_t table_budget) {
+                     const int32_t *out_index, size_t table_budget, bool share_positions) {
   const int variant = ctx->batch_cfg.variant == 4 ? 4 : 3;
   const int warps4 = ctx->batch_cfg.warps_per_cta == 8 ? 8 : 16;
   const int G = variant == 4 ? 16 : kGroups;  // pass capacity in groups (budgeted at this table width)
@@ -822,6 +1027,7 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
     plan.passes.push_back(b);
   }
+  if (share_positions) plan_shared_positions(plan);
   return plan;
 }
 
@@ -850,8 +1056,34 @@ bool fused_each(const FewPass &f) {
 // [row_begin, row_end); row_begin is a multiple of 4096 (the largest block
 // of the pass shapes).  Returns launches.
 int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
-                unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
+                unsigned long long *counts, uint64_t row_begin, uint64_t row_end, void *scratch,
+                size_t scratch_bytes, cudaStream_t s) {
   int launches = 0;
+  // shared positions, when the caller's scratch holds them; else every pass
+  // searches its own
+  const uint64_t pre_rows = row_end > row_begin ? row_end - row_begin : 0;
+  const bool pre = plan.pre.npass > 0 && pre_rows > 0 && scratch &&
+                   (uint64_t)plan.pre.npass * pre_rows * sizeof(uint2) <= scratch_bytes;
+  if (pre) {
+    static std::atomic<uint64_t> raised{0};
+    raise_smem_limit(pre_kernel, raised, 227 * 1024);
+    PreParams P = plan.pre;
+    P.u.blob = dev_blob + plan.pre_off;
+    P.row_begin = row_begin;
+    P.row_end = row_end;
+    P.out = static_cast<uint2 *>(scratch);
+    P.stride = pre_rows;
+    const size_t sm = (size_t)P.u.blob_words * 4;
+    int per = 1;  // resident blocks per SM with this blob
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pre_kernel, kPreThreads, sm) != cudaSuccess || per < 1) {
+      cudaGetLastError();
+      per = 1;
+    }
+    const uint64_t blocks = (pre_rows + kPreThreads * kPreRows - 1) / (kPreThreads * kPreRows);
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)ctx->sm_count * per));
+    pre_kernel<<<grid, kPreThreads, sm, s>>>(P);
+    launches++;
+  }
   for (auto &b : plan.passes) {
     if (b.few && fused_each(b.fp)) {
       // one query (or two over few columns): the single-query scan kernel
@@ -918,7 +1150,11 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.vec_store = (((uintptr_t)out & 15) == 0 && stride_words % 4 == 0) ? 1 : 0;
     bp.word_bytes = 4;
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
-    if (b.variant == 4) {
+    if (pre && b.pre_slot >= 0) {
+      bp.pre = static_cast<const uint2 *>(scratch) + (uint64_t)b.pre_slot * pre_rows;
+      bp.pre_row0 = row_begin;
+      launch_pre4(bp, b.groups, b.warps, ctx->sm_count, s);
+    } else if (b.variant == 4) {
       if (b.cmax == 4) {
         if (b.warps == 8) launch_shape4<4, 8>(bp, b.groups, ctx->sm_count, s);
         else launch_shape4<4, 16>(bp, b.groups, ctx->sm_count, s);
@@ -980,6 +1216,42 @@ const uint32_t *upload_plan(rts_ctx *ctx, const BatchPlan &plan, cudaStream_t s,
   return reinterpret_cast<const uint32_t *>(S.dev);
 }
 
+size_t plan_pre_bytes(const BatchPlan &plan, uint64_t rows) {
+  return (size_t)plan.pre.npass * rows * sizeof(uint2);
+}
+
+// The context's shared-position scratch for `bytes`, ordered after its last
+// use on stream s; null (the passes then search) when the plan needs none or
+// the device has no room (at most an eighth of it is used).
+void *context_pre_scratch(rts_ctx *ctx, size_t bytes, cudaStream_t s) {
+  if (!bytes) return nullptr;
+  if (!ctx->batch) ctx->batch = new BatchScratch();
+  BatchScratch &B = *ctx->batch;
+  if (!B.pre_done) RTS_CUDA(cudaEventCreateWithFlags(&B.pre_done, cudaEventDisableTiming));
+  if (B.pre_cap < bytes) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || bytes > total_b / 8) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    RTS_CUDA(cudaEventSynchronize(B.pre_done));
+    if (B.pre) cudaFree(B.pre);
+    B.pre = nullptr;
+    B.pre_cap = 0;
+    if (cudaMalloc(&B.pre, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    B.pre_cap = bytes;
+  }
+  RTS_CUDA(cudaStreamWaitEvent(s, B.pre_done, 0));
+  return B.pre;
+}
+
+void context_pre_done(rts_ctx *ctx, cudaStream_t s) {
+  if (ctx->batch && ctx->batch->pre_done) RTS_CUDA(cudaEventRecord(ctx->batch->pre_done, s));
+}
+
 void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int nq, uint32_t *out,
                 uint64_t stride_words, unsigned long long *counts, cudaStream_t s, size_t table_budget) {
   std::vector<NormQuery> norm = normalize_all(ctx, terms, offsets, nq);
@@ -989,10 +1261,13 @@ void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int
   RTS_CUDA(cudaMemsetAsync(counts, 0, (size_t)nq * 8, s));
   int launches = launch_outside(ctx, norm, outside, nullptr, out, stride_words, counts, s);
   if (!inside.empty()) {
-    BatchPlan plan = build_plan(ctx, norm, inside, nullptr, table_budget);
+    BatchPlan plan = build_plan(ctx, norm, inside, nullptr, table_budget, true);
     cudaEvent_t done = nullptr;
     const uint32_t *dev_blob = upload_plan(ctx, plan, s, &done);
-    launches += launch_plan(ctx, plan, dev_blob, out, stride_words, counts, 0, ctx->nrows, s);
+    const size_t pre_bytes = plan_pre_bytes(plan, ctx->nrows);
+    void *pre = context_pre_scratch(ctx, pre_bytes, s);
+    launches += launch_plan(ctx, plan, dev_blob, out, stride_words, counts, 0, ctx->nrows, pre, pre_bytes, s);
+    if (pre) context_pre_done(ctx, s);
     RTS_CUDA(cudaEventRecord(done, s));
   }
   RTS_CUDA(cudaGetLastError());
@@ -1002,16 +1277,19 @@ void batch_scan(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int
 void BatchPlanDeleter::operator()(BatchPlan *p) const { delete p; }
 
 BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
-                             const int32_t *out_index, size_t table_budget) {
-  return BatchPlanPtr(new BatchPlan(build_plan(ctx, norm, which, out_index, table_budget)));
+                             const int32_t *out_index, size_t table_budget, bool share_positions) {
+  return BatchPlanPtr(new BatchPlan(build_plan(ctx, norm, which, out_index, table_budget, share_positions)));
 }
 
 const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan) { return plan.blob; }
 
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
-                      unsigned long long *counts, uint64_t row_begin, uint64_t row_end, cudaStream_t s) {
-  return launch_plan(ctx, plan, dev_blob, out, stride_words, counts, row_begin, row_end, s);
+                      unsigned long long *counts, uint64_t row_begin, uint64_t row_end, void *scratch,
+                      size_t scratch_bytes, cudaStream_t s) {
+  return launch_plan(ctx, plan, dev_blob, out, stride_words, counts, row_begin, row_end, scratch, scratch_bytes, s);
 }
+
+size_t batch_plan_scratch_bytes(const BatchPlan &plan, uint64_t rows) { return plan_pre_bytes(plan, rows); }
 
 }  // namespace rts
 
@@ -1121,9 +1399,13 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     rts::BatchPlan plan;
     const uint32_t *dev_blob = nullptr;
     cudaEvent_t blob_done = nullptr;
+    void *pre = nullptr;
+    size_t pre_bytes = 0;
     if (!inside.empty()) {
-      plan = rts::build_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget);
+      plan = rts::build_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget, true);
       dev_blob = rts::upload_plan(ctx, plan, H.compute, &blob_done);
+      pre_bytes = rts::plan_pre_bytes(plan, chunk_rows);
+      pre = rts::context_pre_scratch(ctx, pre_bytes, H.compute);
     }
     for (int r = 0; r < nchunks; r++) {
       const uint64_t r0 = (uint64_t)r * chunk_rows, r1 = std::min<uint64_t>(nrows, r0 + chunk_rows);
@@ -1133,7 +1415,8 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       RTS_CUDA(cudaEventRecord(H.ev[2 * r], H.up));
       RTS_CUDA(cudaStreamWaitEvent(H.compute, H.ev[2 * r], 0));
       if (!inside.empty())
-        ctx->launches += rts::launch_plan(ctx, plan, dev_blob, H.bitmaps, stride_words, H.counts, r0, r1, H.compute);
+        ctx->launches += rts::launch_plan(ctx, plan, dev_blob, H.bitmaps, stride_words, H.counts, r0, r1, pre,
+                                          pre_bytes, H.compute);
       RTS_CUDA(cudaEventRecord(H.ev[2 * r + 1], H.compute));
       RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * r + 1], 0));
       const uint64_t w0 = r0 / 32, w1 = r1 == nrows ? words : r1 / 32;
@@ -1152,6 +1435,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
                                  words * 4, cudaMemcpyDeviceToHost, H.copy));
     }
     if (blob_done) RTS_CUDA(cudaEventRecord(blob_done, H.compute));
+    if (pre) rts::context_pre_done(ctx, H.compute);
     RTS_CUDA(cudaGetLastError());
     if (nq > 0) {
       RTS_CUDA(cudaEventRecord(H.ev[2 * nchunks], H.compute));

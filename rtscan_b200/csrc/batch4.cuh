@@ -101,7 +101,11 @@ __device__ __forceinline__ void transpose32(uint32_t (&x)[32]) {
   }
 }
 
-template <int CMAX, int GV, int W>
+// PRE: the batch's positions were found once for all its passes
+// (pre_kernel in batch.cu), and this pass reads its rows' table word
+// offsets (four uint16 per row) from p.pre instead of searching; only for
+// the shapes that find positions a block ahead.
+template <int CMAX, int GV, int W, bool PRE>
 __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_constant__ BatchPass p) {
   using S = V4Shape<GV, W>;
   constexpr int kV4Threads = S::kThreads;
@@ -136,14 +140,21 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
   // column values are loaded one more block ahead.  Other shapes find the
   // positions of a block in its own step 1.
   constexpr bool kAhead = (GV == 16 || GV == 8) && CMAX <= 4;
-  uint32_t val[S::kRPT][CMAX];                    // column values of this thread's rows
+  static_assert(!PRE || (kAhead && CMAX == 4), "shared positions feed the 4-column look-ahead shapes");
+  uint32_t val[S::kRPT][CMAX];                    // column values of this thread's rows (PRE: packed offsets)
   uint32_t offn[kAhead ? S::kRPT : 1][(CMAX + 1) / 2];  // their table word offsets, two per register
   auto load_values = [&](uint64_t b) {
 #pragma unroll
     for (int h = 0; h < S::kRPT; h++) {
       const uint64_t row = b * S::kRows + threadIdx.x + h * kV4Threads;
+      if (PRE) {  // the row's four offsets, two per word, as find_offsets packs them
+        const uint2 w = row < p.nrows ? __ldg(p.pre + (row - p.pre_row0)) : make_uint2(0u, 0u);
+        val[h][0] = w.x;
+        val[h][1] = w.y;
+      } else {
 #pragma unroll
-      for (int c = 0; c < CMAX; c++) val[h][c] = (c < C && row < p.nrows) ? __ldg(p.col[c] + row) : 0u;
+        for (int c = 0; c < CMAX; c++) val[h][c] = (c < C && row < p.nrows) ? __ldg(p.col[c] + row) : 0u;
+      }
     }
   };
   // kAhead: latency hidden behind the masks, so the search with the fewest
@@ -214,10 +225,16 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
   auto find_offsets = [&](uint64_t b) {  // kAhead: into offn
 #pragma unroll
     for (int h = 0; h < S::kRPT; h++) {
-      uint32_t off[CMAX];
-      row_offsets(b, h, off);
+      if (PRE) {
+        offn[h % (kAhead ? S::kRPT : 1)][0] = val[h][0];
+        offn[h % (kAhead ? S::kRPT : 1)][1 % ((CMAX + 1) / 2)] = val[h][1];
+      } else {
+        uint32_t off[CMAX];
+        row_offsets(b, h, off);
 #pragma unroll
-      for (int c = 0; c < CMAX; c += 2) offn[h % (kAhead ? S::kRPT : 1)][c / 2] = off[c] | (c + 1 < CMAX ? off[c + 1] << 16 : 0u);
+        for (int c = 0; c < CMAX; c += 2)
+          offn[h % (kAhead ? S::kRPT : 1)][c / 2] = off[c] | (c + 1 < CMAX ? off[c + 1] << 16 : 0u);
+      }
     }
   };
   auto put_offsets = [&]() {  // kAhead: from offn

@@ -70,14 +70,23 @@ struct BatchPlanDeleter {
   void operator()(BatchPlan *p) const;
 };
 using BatchPlanPtr = std::unique_ptr<BatchPlan, BatchPlanDeleter>;
+// share_positions: a plan of several table passes over four columns or
+// fewer searches each row's positions once for all of them (a faster step
+// for a little more host planning; the server, whose steps are bound by
+// re-planning at high rates, plans without).
 BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
-                             const int32_t *out_index, size_t table_budget);
+                             const int32_t *out_index, size_t table_budget, bool share_positions);
 // The words to upload to the device before launching.
 const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan);
 // Launch every pass over rows [row_begin, row_end) (row_begin a multiple of
 // 4096) with the plan blob at dev_blob; counts are accumulated (not reset).
+// scratch (scratch_bytes, the caller's, not used by another launch at the
+// same time) holds the rows' shared positions when the plan has them and it
+// is large enough (batch_plan_scratch_bytes); else every pass searches.
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out,
                       uint64_t stride_words, unsigned long long *counts, uint64_t row_begin, uint64_t row_end,
-                      cudaStream_t s);
+                      void *scratch, size_t scratch_bytes, cudaStream_t s);
+// Scratch bytes that launch_batch_plan needs for `rows` rows (0: none).
+size_t batch_plan_scratch_bytes(const BatchPlan &plan, uint64_t rows);
 
 }  // namespace rts

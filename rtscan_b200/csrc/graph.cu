@@ -4,8 +4,9 @@
 // dashboard refresh, a standing query set over a table that is reloaded in
 // place) prepares it once: the host plans the passes, uploads the mask
 // tables, and captures every launch of the batch -- count reset, fill and
-// fused launches for the queries outside the batched kernel, one batched
-// kernel per pass -- into a CUDA graph.  Each rts_batch_launch is then one
+// fused launches for the queries outside the batched kernel, the shared
+// position search when the batch has several passes, one batched kernel per
+// pass -- into a CUDA graph.  Each rts_batch_launch is then one
 // cudaGraphLaunch: no host planning and no per-kernel launch overhead.  The
 // graph reads the context's resident columns at the addresses they had when
 // it was prepared, so it must be re-prepared after the table is reloaded.
@@ -19,6 +20,8 @@
 struct rts_prepared {
   rts_ctx *ctx = nullptr;
   uint32_t *blob = nullptr;
+  void *scratch = nullptr;  // the batch's shared positions (its own: the graph keeps the address)
+  size_t scratch_bytes = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t kernels = 0;  // kernels launched per replay
@@ -26,6 +29,7 @@ struct rts_prepared {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (blob) cudaFree(blob);
+    if (scratch) cudaFree(scratch);
   }
 };
 
@@ -56,13 +60,21 @@ rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t 
     for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
     rts::BatchPlanPtr plan;
     if (!inside.empty()) {
-      plan = rts::make_batch_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget);
+      plan = rts::make_batch_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget, true);
       const auto &blob = rts::batch_plan_blob(*plan);
       if (cudaMalloc(&p->blob, std::max<size_t>(blob.size(), 4) * 4) != cudaSuccess) {
         cudaGetLastError();
         throw rts::Error(RTS_ERR_NOMEM, "plan allocation failed");
       }
       RTS_CUDA(cudaMemcpy(p->blob, blob.data(), blob.size() * 4, cudaMemcpyHostToDevice));
+      // shared positions when there is room (at most an eighth of the device);
+      // without them every pass searches its own
+      const size_t need = rts::batch_plan_scratch_bytes(*plan, ctx->nrows);
+      size_t free_b = 0, total_b = 0;
+      if (need && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need <= total_b / 8 &&
+          cudaMalloc(&p->scratch, need) == cudaSuccess)
+        p->scratch_bytes = need;
+      cudaGetLastError();
     }
     unsigned long long *counts = reinterpret_cast<unsigned long long *>(dev_counts);
     RTS_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
@@ -70,7 +82,9 @@ rts_status rts_batch_prepare(rts_ctx *ctx, const rts_term *terms, const int32_t 
       uint64_t k = 0;
       RTS_CUDA(cudaMemsetAsync(counts, 0, (size_t)nq * 8, s));
       k += rts::launch_outside(ctx, norm, outside, nullptr, dev_bitmaps, stride_words, counts, s);
-      if (plan) k += rts::launch_batch_plan(ctx, *plan, p->blob, dev_bitmaps, stride_words, counts, 0, ctx->nrows, s);
+      if (plan)
+        k += rts::launch_batch_plan(ctx, *plan, p->blob, dev_bitmaps, stride_words, counts, 0, ctx->nrows, p->scratch,
+                                    p->scratch_bytes, s);
       return k;
     };
     // one uncaptured run sets up launch attributes and checks the launches

@@ -236,7 +236,9 @@ struct rts_server {
     if (!plan || plan_slots.empty()) return;
     const uint64_t r0 = (uint64_t)cursor * seg_rows;
     const uint64_t r1 = std::min<uint64_t>(nrows, r0 + seg_rows);
-    ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, stream);
+    // planned without shared positions (re-planning bounds a busy server's
+    // steps, and they cost more host planning), so no scratch
+    ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, nullptr, 0, stream);
     RTS_CUDA(cudaGetLastError());
     cudaEvent_t ev = get_event();
     RTS_CUDA(cudaEventRecord(ev, stream));
@@ -319,7 +321,7 @@ struct rts_server {
           }
         }
         if (todo == 1) {  // plan and upload without the lock
-          rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget);
+          rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget, false);
           upload(rts::batch_plan_blob(*p));
           plan = std::move(p);
           plan_slots = active;

@@ -115,6 +115,63 @@ void check_table_pass(const rts::BatchPlan &plan, const rts::BatchPlan::Pass &b,
   }
 }
 
+uint64_t g_pre_plans = 0, g_pre_lookups = 0;
+
+// Shared positions: for values around every union boundary and at random,
+// the union position (checked against the union bucket index) mapped through
+// each fed pass's table gives the table word offset the pass would find by
+// its own search (tab_off + #{pass boundaries <= x} * groups).
+void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
+  const rts::PreParams &P = plan.pre;
+  if (P.npass == 0) {
+    for (const auto &b : plan.passes) CHECK(b.pre_slot < 0, "a pass fed by shared positions the plan does not have");
+    return;
+  }
+  g_pre_plans++;
+  CHECK(P.npass >= 2 && P.npass <= rts::kMaxPrePasses, "%d passes share positions", P.npass);
+  const uint32_t *ub = plan.blob.data() + plan.pre_off;
+  const uint16_t *lut = reinterpret_cast<const uint16_t *>(ub);
+  int fed = 0;
+  for (const auto &b : plan.passes) {
+    if (b.pre_slot < 0) continue;
+    fed++;
+    const int q = b.pre_slot;
+    CHECK(!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 8, "shared positions feed a pass of shape %d/%d",
+          b.cmax, b.groups);
+    const uint32_t *pblob = plan.blob.data() + b.off;
+    for (int c = 0; c < b.bp.ncols; c++) {
+      const int u = P.ucol[q][c];
+      CHECK(u >= 0 && u < P.u.ncols && P.u.col[u] == b.bp.col[c], "pass column %d maps to union column %d", c, u);
+      if (u < 0 || u >= P.u.ncols) continue;
+      const uint32_t mu = P.u.m[u], mp = b.bp.m[c];
+      const uint32_t *Bu = ub + P.u.bnd_off[u];
+      const uint32_t *Bp = pblob + b.bp.bnd_off[c];
+      std::vector<uint32_t> xs = {0u, kMax};
+      for (uint32_t i = 0; i < mu; i++) {
+        xs.push_back(Bu[i]);
+        if (Bu[i]) xs.push_back(Bu[i] - 1);
+        if (Bu[i] < kMax) xs.push_back(Bu[i] + 1);
+      }
+      for (int r = 0; r < 32; r++) xs.push_back((uint32_t)rng());
+      const uint16_t *bk = reinterpret_cast<const uint16_t *>(ub + P.u.bkt_off[u]);
+      for (uint32_t x : xs) {
+        const uint32_t upos = (uint32_t)(std::upper_bound(Bu, Bu + mu, x) - Bu);
+        if (mu && x >= P.u.bmin[u] && x < P.u.bmax[u]) {
+          const uint32_t v = x - P.u.bmin[u];
+          const uint32_t k = P.u.lgm[u] ? rts::bucket_of(v, P.u.lgm[u]) : v >> P.u.shift[u];
+          CHECK(k < P.u.nbk[u] && bk[k] <= upos && upos <= bk[k + 1], "union column %d value %u: bucket", u, x);
+        }
+        const uint32_t ppos = (uint32_t)(std::upper_bound(Bp, Bp + mp, x) - Bp);
+        const uint32_t want = b.bp.tab_off[c] + ppos * (uint32_t)b.groups;
+        CHECK(lut[P.lut_off[q][c] + upos] == want, "pass %d column %d value %u: offset %u, want %u", q, c, x,
+              lut[P.lut_off[q][c] + upos], want);
+        g_pre_lookups++;
+      }
+    }
+  }
+  CHECK(fed == P.npass, "%d passes fed, %d planned", fed, P.npass);
+}
+
 void check_few_pass(const rts::BatchPlan::Pass &b, const std::vector<rts::NormQuery> &norm, std::vector<int> &seen) {
   const rts::FewPass &f = b.fp;
   g_few_passes++;
@@ -147,14 +204,19 @@ int main(int argc, char **argv) {
   const int counts[] = {1, 2, 3, 4, 20, 21, 32, 100, 128, 129, 200, 256, 257, 400, 512, 513, 700, 1100};
   for (int t = 0; t < trials; t++) {
     auto *ctx = new rts_ctx();  // never destroyed: it owns no device memory
-    const int ncols = 1 + (int)(rng() % 10);
+    // every fifth trial: at most four columns and several passes' worth of
+    // queries, the plans whose passes share positions
+    const bool shared = t % 5 == 4;
+    const int ncols = shared ? 1 + (int)(rng() % 4) : 1 + (int)(rng() % 10);
     for (int c = 0; c < ncols; c++) ctx->cols.push_back(reinterpret_cast<const uint32_t *>(kColStride * (c + 1)));
     ctx->nrows = 1 << 20;
     ctx->sm_count = 148;
     const size_t budgets[] = {136 * 1024, 64 * 1024, 8 * 1024};
     ctx->batch_cfg.table_budget = budgets[rng() % 3];
     ctx->batch_cfg.warps_per_cta = rng() % 2 ? 16 : 8;  // 8-warp passes fit more blob beside a smaller stage
-    const int nq = rng() % 4 ? counts[rng() % (sizeof counts / sizeof counts[0])] : 1 + (int)(rng() % 1100);
+    const int nq = shared   ? 600 + (int)(rng() % 500)
+                   : rng() % 4 ? counts[rng() % (sizeof counts / sizeof counts[0])]
+                               : 1 + (int)(rng() % 1100);
     // bounds from a small pool (shared boundaries, domain edges) and random values
     std::vector<uint32_t> pool = {0, 1, 2, kMax - 1, kMax, 1u << 31};
     for (int i = 0; i < 40; i++) pool.push_back((uint32_t)rng() >> (rng() % 32));
@@ -180,11 +242,12 @@ int main(int argc, char **argv) {
     g_kernel_queries += inside.size();
     std::vector<int> seen(nq, 0);
     if (!inside.empty()) {
-      rts::BatchPlanPtr plan = rts::make_batch_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget);
+      rts::BatchPlanPtr plan = rts::make_batch_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget, true);
       for (const auto &b : plan->passes) {
         if (b.few) check_few_pass(b, norm, seen);
         else check_table_pass(*plan, b, norm, seen, rng);
       }
+      check_pre(*plan, rng);
     }
     for (int q = 0; q < nq; q++) {
       const int want = rts::runs_in_kernel(norm[q]) ? 1 : 0;
@@ -196,8 +259,9 @@ int main(int argc, char **argv) {
     return 1;
   }
   std::printf("planner ok: %d trials, seed %llu: %llu kernel queries, %llu table passes, %llu term-by-term passes, "
-              "%llu mask bits\n",
+              "%llu mask bits, %llu plans with shared positions (%llu lookups)\n",
               trials, (unsigned long long)seed, (unsigned long long)g_kernel_queries, (unsigned long long)g_table_passes,
-              (unsigned long long)g_few_passes, (unsigned long long)g_bits);
+              (unsigned long long)g_few_passes, (unsigned long long)g_bits, (unsigned long long)g_pre_plans,
+              (unsigned long long)g_pre_lookups);
   return 0;
 }

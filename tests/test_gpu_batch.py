@@ -28,9 +28,17 @@ def run_batch(ctx, queries, fn="batch"):
     out = torch.full((max(1, len(queries)) * stride,), -1, dtype=torch.int32, device="cuda")
     cnt = torch.full((max(1, len(queries)),), -1, dtype=torch.int64, device="cuda")
     s = torch.cuda.current_stream().cuda_stream
-    runner = ctx.scan_batch_async if fn == "batch" else ctx.scan_each_async
-    runner(queries, out.data_ptr(), stride, cnt.data_ptr(), s)
-    torch.cuda.synchronize()
+    if fn == "graph":  # prepared once, replayed as a CUDA graph
+        pb = ctx.prepare_batch(queries, out.data_ptr(), stride, cnt.data_ptr())
+        try:
+            pb.launch(s)
+            torch.cuda.synchronize()
+        finally:
+            pb.release()
+    else:
+        runner = ctx.scan_batch_async if fn == "batch" else ctx.scan_each_async
+        runner(queries, out.data_ptr(), stride, cnt.data_ptr(), s)
+        torch.cuda.synchronize()
     o = out.cpu().numpy().view(np.uint32)
     return [(o[i * stride:i * stride + words], int(cnt[i].item()), o[i * stride + words:(i + 1) * stride])
             for i in range(len(queries))]
@@ -334,3 +342,33 @@ def test_prepared_batch_graph_replays_match(ctx, nq):
             assert int(cnt[i].item()) == wcnt, (rep, i)
             assert np.array_equal(o[i * stride:i * stride + words], want), (rep, i)
     pb.release()
+
+
+def test_shared_positions_in_every_path(ctx):
+    """A batch of 1100 queries over four columns plans two 512-slot passes
+    that share one position search per row (and a third, smaller pass that
+    searches on its own).  The plain batch, its CUDA-graph replay, the
+    host-buffer path and the server all give every query's bitmap and count
+    of one query per launch; a sample matches the scalar filter."""
+    n = (1 << 22) + 123
+    cols = [D.zipf(n, 230, 1.1), D.uniform(n, 231), D.normal(n, 232), D.uniform(n, 233, 4096)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 1100, seed=31)
+    want = run_batch(ctx, qs, "each")
+    for runner in ("batch", "graph"):
+        got = run_batch(ctx, qs, runner)
+        for i in range(len(qs)):
+            assert got[i][1] == want[i][1] and np.array_equal(got[i][0], want[i][0]), (runner, i)
+    bms, counts = ctx.scan_batch_host(cols, qs)
+    ctx.load_columns(cols)
+    for i in range(len(qs)):
+        assert int(counts[i]) == want[i][1] and np.array_equal(bms[i, :R.bitmap_words(n)], want[i][0]), ("host", i)
+    with R.Server(ctx, max_active=1100, segment_rows=1 << 20) as srv:
+        tks = [srv.submit(q) for q in qs]
+        for i, tk in enumerate(tks):
+            srv.wait(tk, 120000)
+            bm, cnt = srv.fetch(tk)
+            assert cnt == want[i][1] and np.array_equal(bm, want[i][0]), ("served", i)
+    for i in (0, 511, 512, 1023, 1099):
+        ref, rcnt = expect(cols, qs[i])
+        assert want[i][1] == rcnt and np.array_equal(want[i][0], ref), i
