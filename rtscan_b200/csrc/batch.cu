@@ -130,70 +130,154 @@ __device__ __forceinline__ uint32_t position(const BatchPass &p, const uint32_t 
   return lo;
 }
 
-// Shared positions.  A batch of several table passes searches every row's
-// position once per column, among the union of the passes' boundaries
-// (each pass's boundaries are a subset of the union, so a union position
-// fixes the position in every pass), and maps it through one small table
-// per pass and column to that pass's table word offset.  The passes then
-// read four 16-bit offsets per row instead of searching (batch4_kernel with
-// PRE).
+// Shared positions.  A batch of several table passes over the same columns
+// searches every row's position once per column, among the union of the
+// passes' boundaries (each pass's boundaries are a subset of the union, so
+// a union position fixes the position in every pass), and reads all the
+// passes' table word offsets for it from one entry of a per-column map.
+// The passes then read four 16-bit offsets per row instead of searching
+// (batch4_kernel with PRE).  Pass column c is union column c.
 constexpr int kMaxPrePasses = 4;
+constexpr uint32_t kPreMaxBuckets = 4096;  // per union column
 
-struct PreParams {
-  BatchPass u;                         // the union columns: col, m, bmin, bmax, shift, lgm, bnd_off, bkt_off,
-                                       // nbk, ncols, blob, blob_words
-  uint32_t lut_off[kMaxPrePasses][4];  // pass p, its column c: first entry (in 16-bit units of the blob) of the
-                                       // union position -> table word offset map (m + 1 entries)
-  int32_t ucol[kMaxPrePasses][4];      // union column of pass p's column c (-1: the pass has no column c)
-  int npass;
-  uint64_t row_begin, row_end;
-  uint2 *out;                          // out[p * stride + (row - row_begin)]: four offsets, two per word
-  uint64_t stride;
+// A union column: its m sorted distinct boundaries B, their bucket index and
+// the map.  A value x is clamped to `origin` (B[0] - 1, or 0) and taken
+// relative to it, v = max(x, origin) - origin; its bucket is
+// k = ((s - L) << M) + (v >> s) with s = max(floor(log2 v) - M, L)
+// (floor(log2 0) = -1): buckets of 2^L values below 2^(M+L+1), then 2^M
+// buckets per octave (M = 31: linear buckets only), clamped to nbk - 1.
+// Bucket entry k is base | n << 16: base = #{B <= the bucket's first value},
+// n = #{B in the bucket above its first value} (in the last bucket: every
+// boundary above it), so that pos(x) = base + #{B[base, base + n) <= x},
+// and n = 0 in most buckets.  The map entry of union position p holds the
+// passes' table word offsets for it, two per word (pass 2w in the low half
+// of word w): (npass + 1) / 2 words.
+struct PreCol {
+  const uint32_t *col;
+  uint32_t origin, M, L, nbk, m;
+  uint32_t bkt_off, bnd_off, map_off;  // word offsets into the union blob
 };
 
-__device__ __forceinline__ uint32_t pick4(const uint32_t (&v)[4], int i) {
-  return i == 0 ? v[0] : i == 1 ? v[1] : i == 2 ? v[2] : v[3];
+struct PreParams {
+  PreCol c[4];
+  int ncols;                   // the passes' columns
+  int npass;                   // 2..kMaxPrePasses
+  const uint32_t *blob;        // union blob (global): per column buckets | boundaries | map
+  uint32_t blob_words;
+  uint64_t row_begin, row_end;
+  uint2 *out;                  // out[q * stride + (row - row_begin)]: pass q's four offsets, two per word
+  uint64_t stride;             // pre_stride(row_end - row_begin)
+  int vec;                     // every column 8-byte aligned at row_begin
+};
+
+__host__ __device__ __forceinline__ uint32_t pre_bucket(const PreCol &pc, uint32_t x) {
+  const uint32_t v = (x > pc.origin ? x : pc.origin) - pc.origin;
+#ifdef __CUDA_ARCH__
+  const int e = 31 - __clz(v);  // -1 for v = 0
+#else
+  const int e = v ? 31 - __builtin_clz(v) : -1;
+#endif
+  const int s = e - (int)pc.M > (int)pc.L ? e - (int)pc.M : (int)pc.L;
+  const uint32_t k = (((uint32_t)s - pc.L) << pc.M) + (v >> s);
+  return k < pc.nbk - 1 ? k : pc.nbk - 1;
+}
+
+// Union position of x in column pc: #{B <= x}.
+__host__ __device__ __forceinline__ uint32_t pre_position(const PreCol &pc, const uint32_t *blob, uint32_t x) {
+  const uint32_t w = blob[pc.bkt_off + pre_bucket(pc, x)];
+  uint32_t pos = w & 0xFFFFu, n = w >> 16;
+  const uint32_t *B = blob + pc.bnd_off;
+  while (n) {  // lower bound among B[pos, pos + n)
+    const uint32_t h = n >> 1;
+    if (B[pos + h] <= x) {
+      pos += h + 1;
+      n -= h + 1;
+    } else {
+      n = h;
+    }
+  }
+  return pos;
 }
 
 constexpr int kPreThreads = 512;
-constexpr int kPreRows = 4;  // rows per thread and iteration: their loads and searches overlap
+constexpr int kPrePairs = 2;  // row pairs per thread and iteration: their loads and searches overlap
+constexpr uint64_t kPreTile = (uint64_t)kPreThreads * kPrePairs * 2;  // rows of one block iteration
 
+// Rows of a pass's slice of the scratch: even, so that every pass's slice
+// starts 16-byte aligned and a row pair is one 16-byte store.
+__host__ __device__ __forceinline__ uint64_t pre_stride(uint64_t rows) { return (rows + 1) & ~1ull; }
+
+// U: union columns; NW: map words per entry, 1 for two passes, 2 for three
+// or four.  A thread takes row pairs; tiles wholly inside the range with
+// 8-byte aligned columns (P.vec) load each column's pair as one uint2 and
+// store each pass's pair as one uint4, without per-row checks.
+template <int U, int NW>
 __global__ void __launch_bounds__(kPreThreads) pre_kernel(const __grid_constant__ PreParams P) {
   extern __shared__ __align__(16) uint32_t smem[];
-  for (uint32_t i = threadIdx.x; i < P.u.blob_words; i += blockDim.x) smem[i] = __ldg(P.u.blob + i);
+  for (uint32_t i = threadIdx.x; i < P.blob_words; i += blockDim.x) smem[i] = __ldg(P.blob + i);
   __syncthreads();
-  const uint16_t *lut = reinterpret_cast<const uint16_t *>(smem);
-  const uint64_t tile = (uint64_t)kPreThreads * kPreRows;  // rows of one block iteration
-  for (uint64_t base = P.row_begin + (uint64_t)blockIdx.x * tile; base < P.row_end; base += (uint64_t)gridDim.x * tile) {
-    uint32_t x[kPreRows][4];
+  for (uint64_t base = P.row_begin + (uint64_t)blockIdx.x * kPreTile; base < P.row_end;
+       base += (uint64_t)gridDim.x * kPreTile) {
+    const bool full = P.vec && base + kPreTile <= P.row_end;
+    uint32_t x[kPrePairs][2][U];
 #pragma unroll
-    for (int r = 0; r < kPreRows; r++) {
-      const uint64_t row = base + threadIdx.x + (uint64_t)r * kPreThreads;
+    for (int j = 0; j < kPrePairs; j++) {
+      const uint64_t row = base + 2 * (threadIdx.x + (uint64_t)j * kPreThreads);
 #pragma unroll
-      for (int u = 0; u < 4; u++) x[r][u] = (u < P.u.ncols && row < P.row_end) ? __ldg(P.u.col[u] + row) : 0u;
+      for (int c = 0; c < U; c++) {
+        if (full) {
+          const uint2 v = __ldg(reinterpret_cast<const uint2 *>(P.c[c].col + row));
+          x[j][0][c] = v.x;
+          x[j][1][c] = v.y;
+        } else {
+          x[j][0][c] = row < P.row_end ? __ldg(P.c[c].col + row) : 0u;
+          x[j][1][c] = row + 1 < P.row_end ? __ldg(P.c[c].col + row + 1) : 0u;
+        }
+      }
     }
-    // the searches of the thread's rows and columns are independent, so
-    // their shared-memory loads overlap (a loop-free lookup with a fallback
-    // search, or eight rows per thread, measured slower)
-    uint32_t pos[kPreRows][4];
+    // map entries of every row and column; the searches of the thread's rows
+    // and columns are independent, so their shared-memory loads overlap
+    uint32_t e[kPrePairs][2][4][NW];
 #pragma unroll
-    for (int r = 0; r < kPreRows; r++)
+    for (int j = 0; j < kPrePairs; j++)
 #pragma unroll
-      for (int u = 0; u < 4; u++) pos[r][u] = u < P.u.ncols ? position(P.u, smem, u, x[r][u]) : 0u;
-#pragma unroll
-    for (int r = 0; r < kPreRows; r++) {
-      const uint64_t row = base + threadIdx.x + (uint64_t)r * kPreThreads;
-      if (row >= P.row_end) continue;
-#pragma unroll
-      for (int q = 0; q < kMaxPrePasses; q++) {
-        if (q >= P.npass) break;
-        uint32_t o[4];
+      for (int h = 0; h < 2; h++)
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          const int u = P.ucol[q][c];
-          o[c] = u >= 0 ? lut[P.lut_off[q][c] + pick4(pos[r], u)] : 0u;
+          if (c < U) {
+            const uint32_t *ent = smem + P.c[c].map_off + pre_position(P.c[c], smem, x[j][h][c]) * NW;
+            if (NW == 2) {
+              const uint2 w = *reinterpret_cast<const uint2 *>(ent);
+              e[j][h][c][0] = w.x;
+              e[j][h][c][NW - 1] = w.y;
+            } else {
+              e[j][h][c][0] = *ent;
+            }
+          } else {
+#pragma unroll
+            for (int w = 0; w < NW; w++) e[j][h][c][w] = 0u;
+          }
         }
-        P.out[q * P.stride + (row - P.row_begin)] = make_uint2(o[0] | (o[1] << 16), o[2] | (o[3] << 16));
+#pragma unroll
+    for (int j = 0; j < kPrePairs; j++) {
+      const uint64_t row = base + 2 * (threadIdx.x + (uint64_t)j * kPreThreads);
+#pragma unroll
+      for (int q = 0; q < 2 * NW; q++) {
+        if (q >= P.npass) break;
+        const int w = q >> 1;
+        const uint32_t sel = (q & 1) ? 0x7632u : 0x5410u;  // the pass's halves of two entries
+        uint2 o[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+          o[h] = make_uint2(__byte_perm(e[j][h][0][w], e[j][h][1][w], sel),
+                            __byte_perm(e[j][h][2][w], e[j][h][3][w], sel));
+        uint2 *dst = P.out + q * P.stride + (row - P.row_begin);
+        if (full) {
+          *reinterpret_cast<uint4 *>(dst) = make_uint4(o[0].x, o[0].y, o[1].x, o[1].y);
+        } else {
+          if (row < P.row_end) dst[0] = o[0];
+          if (row + 1 < P.row_end) dst[1] = o[1];
+        }
       }
     }
   }
@@ -765,113 +849,187 @@ bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && 
 // Slot groups of a variant-4 pass of nq queries.
 int pass_groups(int nq) { return nq <= 128 ? 4 : nq <= 256 ? 8 : 16; }
 
+// Start of bucket k of a union column, relative to its origin (inverse of
+// pre_bucket below the clamp).
+uint64_t pre_bucket_start(uint32_t M, uint32_t L, uint32_t k) {
+  if ((k >> M) <= 1) return (uint64_t)k << L;  // linear part
+  const uint32_t t = (k >> M) - 1;
+  const uint64_t w = (k & ((1u << M) - 1)) | (1u << M);
+  return w << (t + L);
+}
+
+// Bucket index of a union column (PreCol) with at most kPreMaxBuckets
+// buckets.  Candidates: linear buckets, and for M = 1..12 the log-linear
+// ones with the smallest L that fits; the one whose boundaries need the
+// fewest search steps in all wins (the query bounds sit where the rows
+// are dense), fewer buckets on a tie.
+std::vector<uint32_t> pre_buckets(const std::vector<uint32_t> &B, PreCol &pc) {
+  const uint32_t m = (uint32_t)B.size();
+  pc.m = m;
+  pc.origin = m && B[0] > 0 ? B[0] - 1 : 0;
+  if (m == 0) {
+    pc.M = 31;
+    pc.L = 0;
+    pc.nbk = 1;
+    return {0u};
+  }
+  auto entries = [&](uint32_t M, uint32_t L, uint32_t nbk, double *cost) {
+    PreCol t = pc;
+    t.M = M;
+    t.L = L;
+    t.nbk = nbk;
+    std::vector<uint32_t> ent(nbk);
+    std::vector<uint32_t> first(nbk + 1, m);  // first boundary whose bucket is >= k
+    for (uint32_t i = m; i-- > 0;) first[pre_bucket(t, B[i])] = i;
+    for (uint32_t k = nbk; k-- > 0;) first[k] = std::min(first[k], first[k + 1]);
+    *cost = 0;
+    for (uint32_t k = 0; k < nbk; k++) {
+      const uint32_t lo = first[k], hi = k + 1 < nbk ? first[k + 1] : m;
+      const uint64_t start = (uint64_t)pc.origin + pre_bucket_start(M, L, k);
+      const uint32_t base = lo + (lo < hi && B[lo] == start ? 1u : 0u);
+      const uint32_t n = hi - base;
+      ent[k] = base | n << 16;
+      uint32_t steps = 0;
+      for (uint32_t r = n; r; r >>= 1) steps++;
+      *cost += (double)steps * (hi - lo);
+    }
+    return ent;
+  };
+  const uint32_t vmax = B.back() - pc.origin;
+  struct Cand {
+    uint32_t M, L, nbk;
+  };
+  std::vector<Cand> cands;
+  {
+    uint32_t L = 0;
+    while ((vmax >> L) >= kPreMaxBuckets) L++;
+    cands.push_back({31, L, (vmax >> L) + 1});
+  }
+  for (uint32_t M = 1; M <= 12; M++)
+    for (uint32_t L = 0; L < 32; L++) {
+      PreCol t = pc;
+      t.M = M;
+      t.L = L;
+      t.nbk = 0xFFFFFFFFu;
+      const uint32_t nbk = pre_bucket(t, B.back()) + 1;
+      if (nbk <= kPreMaxBuckets) {
+        cands.push_back({M, L, nbk});
+        break;
+      }
+    }
+  std::vector<uint32_t> best;
+  double best_cost = 0;
+  for (const Cand &cd : cands) {
+    double cost;
+    std::vector<uint32_t> ent = entries(cd.M, cd.L, cd.nbk, &cost);
+    if (best.empty() || cost < best_cost || (cost == best_cost && ent.size() < best.size())) {
+      best = std::move(ent);
+      best_cost = cost;
+      pc.M = cd.M;
+      pc.L = cd.L;
+      pc.nbk = cd.nbk;
+    }
+  }
+  return best;
+}
+
+// Move column s of `src` to column c of `dst` (a pass's per-column fields).
+void move_column(BatchPass &dst, int c, const BatchPass &src, int s) {
+  dst.col[c] = src.col[s];
+  dst.m[c] = src.m[s];
+  dst.bmin[c] = src.bmin[s];
+  dst.bmax[c] = src.bmax[s];
+  dst.shift[c] = src.shift[s];
+  dst.lgm[c] = src.lgm[s];
+  dst.tab_off[c] = src.tab_off[s];
+  dst.bnd_off[c] = src.bnd_off[s];
+  dst.bkt_off[c] = src.bkt_off[s];
+  dst.nbk[c] = src.nbk[s];
+}
+
 // Shared positions for a plan with at least two table passes of the
-// look-ahead shapes (256 or 512 slots) over four columns or fewer whose
-// columns together are at most four: the union of their boundaries per
-// column with its bucket index, and per pass and column the map from a
-// union position to the pass's table word offset (a pass's boundaries are
-// a subset of the union, so the pass position of union position k is the
-// number of its boundaries <= B_u[k-1]).  Appended to the plan blob; other
-// plans are left as they are.
+// look-ahead shapes (256 or 512 slots, at most four columns) over the same
+// columns: the later passes' columns are put in the first one's order; per
+// column the union of the passes' boundaries with its bucket index, and
+// the map from a union position to every pass's table word offset (a
+// pass's boundaries are a subset of the union, so the pass position of
+// union position k is the number of its boundaries <= B_u[k-1]).  Appended
+// to the plan blob; other plans are left as they are.
 void plan_shared_positions(BatchPlan &plan) {
   plan.pre.npass = 0;
   std::vector<int> which;
-  for (size_t i = 0; i < plan.passes.size(); i++) {
+  for (size_t i = 0; i < plan.passes.size() && (int)which.size() < kMaxPrePasses; i++) {
     const BatchPlan::Pass &b = plan.passes[i];
-    if (!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 8 && (int)which.size() < kMaxPrePasses)
-      which.push_back((int)i);
+    if (b.few || b.variant != 4 || b.cmax != 4 || b.groups < 8) continue;
+    if (!which.empty()) {
+      const BatchPass &f = plan.passes[which[0]].bp;
+      if (b.bp.ncols != f.ncols) continue;
+      bool same = true;
+      for (int c = 0; c < f.ncols; c++) same = same && std::find(b.bp.col, b.bp.col + b.bp.ncols, f.col[c]) != b.bp.col + b.bp.ncols;
+      if (!same) continue;
+    }
+    which.push_back((int)i);
   }
   if (which.size() < 2) return;
-  std::vector<const uint32_t *> ucols;
-  for (int i : which) {
-    const BatchPass &bp = plan.passes[i].bp;
-    for (int c = 0; c < bp.ncols; c++)
-      if (std::find(ucols.begin(), ucols.end(), bp.col[c]) == ucols.end()) ucols.push_back(bp.col[c]);
-  }
-  if (ucols.size() > 4) return;
-  const int U = (int)ucols.size();
+  const int U = plan.passes[which[0]].bp.ncols;
+  const int npass = (int)which.size(), NW = (npass + 1) / 2;
   std::vector<std::vector<uint32_t>> Bu(U);
-  for (int i : which) {
-    const BatchPlan::Pass &b = plan.passes[i];
-    const uint32_t *blob = plan.blob.data() + b.off;
-    for (int c = 0; c < b.bp.ncols; c++) {
-      const int u = (int)(std::find(ucols.begin(), ucols.end(), b.bp.col[c]) - ucols.begin());
-      Bu[u].insert(Bu[u].end(), blob + b.bp.bnd_off[c], blob + b.bp.bnd_off[c] + b.bp.m[c]);
+  std::vector<BatchPass> ordered(npass);
+  for (int q = 0; q < npass; q++) {
+    const BatchPass &src = plan.passes[which[q]].bp;
+    ordered[q] = src;
+    for (int c = 0; c < U; c++) {
+      const int s = (int)(std::find(src.col, src.col + U, plan.passes[which[0]].bp.col[c]) - src.col);
+      move_column(ordered[q], c, src, s);
     }
+    const uint32_t *blob = plan.blob.data() + plan.passes[which[q]].off;
+    for (int c = 0; c < U; c++)
+      Bu[c].insert(Bu[c].end(), blob + ordered[q].bnd_off[c], blob + ordered[q].bnd_off[c] + ordered[q].m[c]);
   }
-  for (auto &B : Bu) {
+  PreParams P;
+  memset(&P, 0, sizeof P);
+  P.ncols = U;
+  P.npass = npass;
+  std::vector<uint32_t> ub;  // offsets relative to its own start
+  for (int c = 0; c < U; c++) {
+    std::vector<uint32_t> &B = Bu[c];
     std::sort(B.begin(), B.end());
     B.erase(std::unique(B.begin(), B.end()), B.end());
-    if (B.size() > 0xFFFEu) return;  // positions are 16-bit
-  }
-  PreParams &P = plan.pre;
-  memset(&P, 0, sizeof P);
-  std::vector<uint32_t> blob;  // boundaries | buckets | maps, offsets relative to its own start
-  BatchPass &u = P.u;
-  u.ncols = U;
-  for (int c = 0; c < U; c++) {
-    u.col[c] = ucols[c];
-    const uint32_t m = (uint32_t)Bu[c].size();
-    u.m[c] = m;
-    u.bnd_off[c] = (uint32_t)blob.size();
-    blob.insert(blob.end(), Bu[c].begin(), Bu[c].end());
-    if (m == 0) {
-      u.bkt_off[c] = (uint32_t)blob.size();
-      u.nbk[c] = 1;
-      blob.push_back(0);
-      continue;
-    }
-    u.bmin[c] = Bu[c].front();
-    u.bmax[c] = Bu[c].back();
-    uint32_t nb = 1;
-    while (nb < 16 * m && nb < 4096) nb <<= 1;
-    const uint64_t span = (uint64_t)u.bmax[c] - u.bmin[c] + 1;
-    const std::vector<uint16_t> bk = bucket_index(Bu[c], span, nb, &u.shift[c], &u.lgm[c]);
-    u.nbk[c] = (uint32_t)bk.size() - 1;
-    u.bkt_off[c] = (uint32_t)blob.size();
-    blob.resize(blob.size() + (bk.size() + 1) / 2, 0u);
-    memcpy(blob.data() + u.bkt_off[c], bk.data(), bk.size() * 2);
-  }
-  std::vector<uint16_t> maps;  // appended after the words above
-  for (int q = 0; q < (int)which.size(); q++) {
-    BatchPlan::Pass &b = plan.passes[which[q]];
-    const uint32_t *pblob = plan.blob.data() + b.off;
-    for (int c = 0; c < 4; c++) {
-      P.ucol[q][c] = -1;
-      if (c >= b.bp.ncols) continue;
-      const int uc = (int)(std::find(ucols.begin(), ucols.end(), b.bp.col[c]) - ucols.begin());
-      P.ucol[q][c] = uc;
-      P.lut_off[q][c] = (uint32_t)(blob.size() * 2 + maps.size());
-      const uint32_t *Bp = pblob + b.bp.bnd_off[c];
-      const uint32_t mp = b.bp.m[c];
-      const std::vector<uint32_t> &B = Bu[uc];
+    if (B.size() > 0xFFFFu) return;  // bucket entries hold 16-bit positions
+    PreCol &pc = P.c[c];
+    pc.col = ordered[0].col[c];
+    const std::vector<uint32_t> ent = pre_buckets(B, pc);
+    pc.bkt_off = (uint32_t)ub.size();
+    ub.insert(ub.end(), ent.begin(), ent.end());
+    pc.bnd_off = (uint32_t)ub.size();
+    ub.insert(ub.end(), B.begin(), B.end());
+    if (NW == 2 && ub.size() % 2) ub.push_back(0);  // 8-byte map entries
+    pc.map_off = (uint32_t)ub.size();
+    ub.resize(ub.size() + (B.size() + 1) * NW, 0u);
+    for (int q = 0; q < npass; q++) {
+      const BatchPlan::Pass &b = plan.passes[which[q]];
+      const uint32_t *Bp = plan.blob.data() + b.off + ordered[q].bnd_off[c];
+      const uint32_t mp = ordered[q].m[c];
       uint32_t j = 0;
       for (size_t k = 0; k <= B.size(); k++) {
         if (k > 0)
           while (j < mp && Bp[j] <= B[k - 1]) j++;
-        const uint64_t off = (uint64_t)b.bp.tab_off[c] + (uint64_t)j * b.groups;
-        if (off > 0xFFFFu) {  // table offsets are 16-bit in the maps
-          plan.pre.npass = 0;
-          return;
-        }
-        maps.push_back((uint16_t)off);
+        const uint64_t off = (uint64_t)ordered[q].tab_off[c] + (uint64_t)j * b.groups;
+        if (off > 0xFFFFu) return;  // table offsets are 16-bit in the map
+        ub[pc.map_off + k * NW + q / 2] |= (uint32_t)off << (16 * (q & 1));
       }
     }
   }
-  if (maps.size() & 1) maps.push_back(0);
-  const size_t words = blob.size();
-  blob.resize(words + maps.size() / 2);
-  memcpy(blob.data() + words, maps.data(), maps.size() * 2);
-  if (blob.size() * 4 > 200 * 1024) {  // the pre kernel's shared memory
-    plan.pre.npass = 0;
-    return;
+  if (ub.size() * 4 > 200 * 1024) return;  // the pre kernel's shared memory
+  P.blob_words = (uint32_t)ub.size();
+  plan.pre = P;
+  for (int q = 0; q < npass; q++) {
+    plan.passes[which[q]].bp = ordered[q];
+    plan.passes[which[q]].pre_slot = q;
   }
-  u.blob_words = (uint32_t)blob.size();
-  P.npass = (int)which.size();
-  for (int q = 0; q < P.npass; q++) plan.passes[which[q]].pre_slot = q;
   while (plan.blob.size() % 4) plan.blob.push_back(0);
   plan.pre_off = plan.blob.size();
-  plan.blob.insert(plan.blob.end(), blob.begin(), blob.end());
+  plan.blob.insert(plan.blob.end(), ub.begin(), ub.end());
 }
 
 // Passes for the kernel queries `which` (indices into norm); query qi writes
@@ -1052,6 +1210,43 @@ bool fused_each(const FewPass &f) {
   return f.nq == 1 || terms <= 6;
 }
 
+// The pre kernel over P's rows, one block per SM and resident slot.
+template <int U, int NW>
+void launch_pre_shape(rts_ctx *ctx, const PreParams &P, cudaStream_t s) {
+  static std::atomic<uint64_t> raised{0};
+  raise_smem_limit(pre_kernel<U, NW>, raised, 227 * 1024);
+  const size_t sm = (size_t)P.blob_words * 4;
+  int per = 1;  // resident blocks per SM with this blob
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pre_kernel<U, NW>, kPreThreads, sm) != cudaSuccess ||
+      per < 1) {
+    cudaGetLastError();
+    per = 1;
+  }
+  const uint64_t blocks = (P.row_end - P.row_begin + kPreTile - 1) / kPreTile;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)ctx->sm_count * per));
+  pre_kernel<U, NW><<<grid, kPreThreads, sm, s>>>(P);
+}
+
+template <int NW>
+void launch_pre_nw(rts_ctx *ctx, const PreParams &P, cudaStream_t s) {
+  switch (P.ncols) {
+    case 1: launch_pre_shape<1, NW>(ctx, P, s); break;
+    case 2: launch_pre_shape<2, NW>(ctx, P, s); break;
+    case 3: launch_pre_shape<3, NW>(ctx, P, s); break;
+    default: launch_pre_shape<4, NW>(ctx, P, s); break;
+  }
+}
+
+void launch_pre(rts_ctx *ctx, PreParams P, cudaStream_t s) {
+  P.stride = pre_stride(P.row_end - P.row_begin);
+  P.vec = ((uintptr_t)P.out & 15) == 0;
+  for (int c = 0; c < P.ncols; c++) P.vec = P.vec && ((uintptr_t)(P.c[c].col + P.row_begin) & 7) == 0;
+  if (P.npass <= 2)
+    launch_pre_nw<1>(ctx, P, s);
+  else
+    launch_pre_nw<2>(ctx, P, s);
+}
+
 // Launch every pass of `plan` (blob already on the device) over rows
 // [row_begin, row_end); row_begin is a multiple of 4096 (the largest block
 // of the pass shapes).  Returns launches.
@@ -1063,25 +1258,14 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
   // searches its own
   const uint64_t pre_rows = row_end > row_begin ? row_end - row_begin : 0;
   const bool pre = plan.pre.npass > 0 && pre_rows > 0 && scratch &&
-                   (uint64_t)plan.pre.npass * pre_rows * sizeof(uint2) <= scratch_bytes;
+                   (uint64_t)plan.pre.npass * pre_stride(pre_rows) * sizeof(uint2) <= scratch_bytes;
   if (pre) {
-    static std::atomic<uint64_t> raised{0};
-    raise_smem_limit(pre_kernel, raised, 227 * 1024);
     PreParams P = plan.pre;
-    P.u.blob = dev_blob + plan.pre_off;
+    P.blob = dev_blob + plan.pre_off;
     P.row_begin = row_begin;
     P.row_end = row_end;
     P.out = static_cast<uint2 *>(scratch);
-    P.stride = pre_rows;
-    const size_t sm = (size_t)P.u.blob_words * 4;
-    int per = 1;  // resident blocks per SM with this blob
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pre_kernel, kPreThreads, sm) != cudaSuccess || per < 1) {
-      cudaGetLastError();
-      per = 1;
-    }
-    const uint64_t blocks = (pre_rows + kPreThreads * kPreRows - 1) / (kPreThreads * kPreRows);
-    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)ctx->sm_count * per));
-    pre_kernel<<<grid, kPreThreads, sm, s>>>(P);
+    launch_pre(ctx, P, s);
     launches++;
   }
   for (auto &b : plan.passes) {
@@ -1151,7 +1335,7 @@ int launch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_
     bp.word_bytes = 4;
     const bool w8 = ctx->batch_cfg.warps_per_cta == 8;
     if (pre && b.pre_slot >= 0) {
-      bp.pre = static_cast<const uint2 *>(scratch) + (uint64_t)b.pre_slot * pre_rows;
+      bp.pre = static_cast<const uint2 *>(scratch) + (uint64_t)b.pre_slot * pre_stride(pre_rows);
       bp.pre_row0 = row_begin;
       launch_pre4(bp, b.groups, b.warps, ctx->sm_count, s);
     } else if (b.variant == 4) {
@@ -1217,7 +1401,7 @@ const uint32_t *upload_plan(rts_ctx *ctx, const BatchPlan &plan, cudaStream_t s,
 }
 
 size_t plan_pre_bytes(const BatchPlan &plan, uint64_t rows) {
-  return (size_t)plan.pre.npass * rows * sizeof(uint2);
+  return (size_t)plan.pre.npass * pre_stride(rows) * sizeof(uint2);
 }
 
 // The context's shared-position scratch for `bytes`, ordered after its last

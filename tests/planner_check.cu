@@ -121,6 +121,34 @@ uint64_t g_pre_plans = 0, g_pre_lookups = 0;
 // the union position (checked against the union bucket index) mapped through
 // each fed pass's table gives the table word offset the pass would find by
 // its own search (tab_off + #{pass boundaries <= x} * groups).
+// Values to look up in a union column: both domain ends, every boundary and
+// its neighbours, and random values.
+std::vector<uint32_t> probe_values(const uint32_t *B, uint32_t m, std::mt19937_64 &rng) {
+  std::vector<uint32_t> xs = {0u, 1u, kMax - 1, kMax};
+  for (uint32_t i = 0; i < m; i++) {
+    xs.push_back(B[i]);
+    if (B[i]) xs.push_back(B[i] - 1);
+    if (B[i] < kMax) xs.push_back(B[i] + 1);
+  }
+  for (int r = 0; r < 64; r++) xs.push_back((uint32_t)rng() >> (rng() % 32));
+  return xs;
+}
+
+// The bucket index of one union column: pre_position equals the number of
+// boundaries <= x for every probe value.
+void check_pre_column(const rts::PreCol &pc, const uint32_t *ub, std::mt19937_64 &rng) {
+  const uint32_t *B = ub + pc.bnd_off;
+  CHECK(pc.nbk >= 1 && pc.nbk <= rts::kPreMaxBuckets, "union column with %u buckets", pc.nbk);
+  for (uint32_t i = 1; i < pc.m; i++) CHECK(B[i - 1] < B[i], "union boundaries not sorted and distinct");
+  for (uint32_t x : probe_values(B, pc.m, rng)) {
+    const uint32_t want = (uint32_t)(std::upper_bound(B, B + pc.m, x) - B);
+    const uint32_t got = rts::pre_position(pc, ub, x);
+    CHECK(got == want, "union column (M %u L %u origin %u, %u buckets, m %u) value %u: position %u, want %u", pc.M,
+          pc.L, pc.origin, pc.nbk, pc.m, x, got, want);
+    g_pre_lookups++;
+  }
+}
+
 void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
   const rts::PreParams &P = plan.pre;
   if (P.npass == 0) {
@@ -129,47 +157,64 @@ void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
   }
   g_pre_plans++;
   CHECK(P.npass >= 2 && P.npass <= rts::kMaxPrePasses, "%d passes share positions", P.npass);
+  CHECK(P.ncols >= 1 && P.ncols <= 4, "%d union columns", P.ncols);
   const uint32_t *ub = plan.blob.data() + plan.pre_off;
-  const uint16_t *lut = reinterpret_cast<const uint16_t *>(ub);
+  const int NW = (P.npass + 1) / 2;
+  CHECK(P.blob_words * 4 <= 200 * 1024 && plan.pre_off + P.blob_words <= plan.blob.size(), "union blob of %u words",
+        P.blob_words);
+  for (int c = 0; c < P.ncols; c++) check_pre_column(P.c[c], ub, rng);
   int fed = 0;
   for (const auto &b : plan.passes) {
     if (b.pre_slot < 0) continue;
     fed++;
     const int q = b.pre_slot;
+    CHECK(q < P.npass, "pass slot %d of %d", q, P.npass);
     CHECK(!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 8, "shared positions feed a pass of shape %d/%d",
           b.cmax, b.groups);
+    CHECK(b.bp.ncols == P.ncols, "a pass of %d columns fed by %d union columns", b.bp.ncols, P.ncols);
     const uint32_t *pblob = plan.blob.data() + b.off;
-    for (int c = 0; c < b.bp.ncols; c++) {
-      const int u = P.ucol[q][c];
-      CHECK(u >= 0 && u < P.u.ncols && P.u.col[u] == b.bp.col[c], "pass column %d maps to union column %d", c, u);
-      if (u < 0 || u >= P.u.ncols) continue;
-      const uint32_t mu = P.u.m[u], mp = b.bp.m[c];
-      const uint32_t *Bu = ub + P.u.bnd_off[u];
+    for (int c = 0; c < b.bp.ncols && c < P.ncols; c++) {
+      const rts::PreCol &pc = P.c[c];
+      CHECK(pc.col == b.bp.col[c], "pass column %d is not union column %d", c, c);
+      const uint32_t *Bu = ub + pc.bnd_off;
       const uint32_t *Bp = pblob + b.bp.bnd_off[c];
-      std::vector<uint32_t> xs = {0u, kMax};
-      for (uint32_t i = 0; i < mu; i++) {
-        xs.push_back(Bu[i]);
-        if (Bu[i]) xs.push_back(Bu[i] - 1);
-        if (Bu[i] < kMax) xs.push_back(Bu[i] + 1);
-      }
-      for (int r = 0; r < 32; r++) xs.push_back((uint32_t)rng());
-      const uint16_t *bk = reinterpret_cast<const uint16_t *>(ub + P.u.bkt_off[u]);
-      for (uint32_t x : xs) {
-        const uint32_t upos = (uint32_t)(std::upper_bound(Bu, Bu + mu, x) - Bu);
-        if (mu && x >= P.u.bmin[u] && x < P.u.bmax[u]) {
-          const uint32_t v = x - P.u.bmin[u];
-          const uint32_t k = P.u.lgm[u] ? rts::bucket_of(v, P.u.lgm[u]) : v >> P.u.shift[u];
-          CHECK(k < P.u.nbk[u] && bk[k] <= upos && upos <= bk[k + 1], "union column %d value %u: bucket", u, x);
-        }
+      const uint32_t mp = b.bp.m[c];
+      for (uint32_t x : probe_values(Bu, pc.m, rng)) {
+        const uint32_t upos = (uint32_t)(std::upper_bound(Bu, Bu + pc.m, x) - Bu);
         const uint32_t ppos = (uint32_t)(std::upper_bound(Bp, Bp + mp, x) - Bp);
         const uint32_t want = b.bp.tab_off[c] + ppos * (uint32_t)b.groups;
-        CHECK(lut[P.lut_off[q][c] + upos] == want, "pass %d column %d value %u: offset %u, want %u", q, c, x,
-              lut[P.lut_off[q][c] + upos], want);
+        const uint32_t got = (ub[pc.map_off + upos * NW + q / 2] >> (16 * (q & 1))) & 0xFFFFu;
+        CHECK(got == want, "pass %d column %d value %u: offset %u, want %u", q, c, x, got, want);
         g_pre_lookups++;
       }
     }
   }
   CHECK(fed == P.npass, "%d passes fed, %d planned", fed, P.npass);
+}
+
+// Bucket indexes of crafted boundary sets: single boundaries at the domain
+// ends, dense runs, wide spreads, and runs crowded into one octave.
+void check_pre_buckets(std::mt19937_64 &rng) {
+  std::vector<std::vector<uint32_t>> sets = {
+      {0}, {1}, {kMax}, {0, kMax}, {0, 1, 2, 3}, {kMax - 3, kMax - 2, kMax - 1, kMax}, {1u << 31}};
+  std::vector<uint32_t> dense, wide, octave, skew, big;
+  for (uint32_t i = 0; i < 3000; i++) dense.push_back(1000 + i);
+  for (uint32_t i = 0; i < 2000; i++) wide.push_back((uint32_t)rng());
+  for (uint32_t i = 0; i < 1500; i++) octave.push_back((1u << 30) + (uint32_t)(rng() % (1u << 20)));
+  for (uint32_t i = 0; i < 2500; i++) skew.push_back((uint32_t)rng() >> (rng() % 32));
+  for (uint32_t i = 0; i < 65535; i++) big.push_back(i * 65537u);
+  for (auto *v : {&dense, &wide, &octave, &skew, &big}) sets.push_back(*v);
+  for (auto &B : sets) {
+    std::sort(B.begin(), B.end());
+    B.erase(std::unique(B.begin(), B.end()), B.end());
+    rts::PreCol pc;
+    std::memset(&pc, 0, sizeof pc);
+    std::vector<uint32_t> ub = rts::pre_buckets(B, pc);
+    pc.bkt_off = 0;
+    pc.bnd_off = (uint32_t)ub.size();
+    ub.insert(ub.end(), B.begin(), B.end());
+    check_pre_column(pc, ub.data(), rng);
+  }
 }
 
 void check_few_pass(const rts::BatchPlan::Pass &b, const std::vector<rts::NormQuery> &norm, std::vector<int> &seen) {
@@ -201,6 +246,7 @@ int main(int argc, char **argv) {
   const uint64_t seed = argc > 1 ? std::strtoull(argv[1], nullptr, 10) : 1;
   const int trials = argc > 2 ? std::atoi(argv[2]) : 20;
   std::mt19937_64 rng(seed);
+  check_pre_buckets(rng);
   const int counts[] = {1, 2, 3, 4, 20, 21, 32, 100, 128, 129, 200, 256, 257, 400, 512, 513, 700, 1100};
   for (int t = 0; t < trials; t++) {
     auto *ctx = new rts_ctx();  // never destroyed: it owns no device memory
@@ -219,7 +265,10 @@ int main(int argc, char **argv) {
                                : 1 + (int)(rng() % 1100);
     // bounds from a small pool (shared boundaries, domain edges) and random values
     std::vector<uint32_t> pool = {0, 1, 2, kMax - 1, kMax, 1u << 31};
-    for (int i = 0; i < 40; i++) pool.push_back((uint32_t)rng() >> (rng() % 32));
+    // (every tenth trial a pool of 1500, so that the union columns hold
+    // hundreds of boundaries, crowded buckets among them)
+    const int npool = shared && t % 10 == 9 ? 1500 : 40;
+    for (int i = 0; i < npool; i++) pool.push_back((uint32_t)rng() >> (rng() % 32));
     std::vector<rts_term> terms;
     std::vector<int32_t> offsets = {0};
     for (int q = 0; q < nq; q++) {

@@ -372,3 +372,16 @@ def test_shared_positions_in_every_path(ctx):
     for i in (0, 511, 512, 1023, 1099):
         ref, rcnt = expect(cols, qs[i])
         assert want[i][1] == rcnt and np.array_equal(want[i][0], ref), i
+    # columns attached 4 bytes past an 8-byte boundary: the position search
+    # loads one row at a time
+    held = []
+    for c in cols:
+        t = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        t[1:] = torch.from_numpy(c.view(np.int32)).cuda()
+        held.append(t)
+    ctx.attach_columns([t.data_ptr() + 4 for t in held], n)
+    got = run_batch(ctx, qs, "batch")
+    for i in range(len(qs)):
+        assert got[i][1] == want[i][1] and np.array_equal(got[i][0], want[i][0]), ("unaligned", i)
+    ctx.load_columns(cols)
+    del held
