@@ -125,30 +125,34 @@ def host_info():
     return {"host_cpus": os.cpu_count(), "cpu_model": model}
 
 
-# DRAM traffic of the dominant kernel from one ncu capture each
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch) beside that
-# launch's own bytes: columns read once and one bitmap written per query of
-# the launch.  A launch of the timed workload is credited with the same
-# traffic-to-bytes ratio (the kernel streams each column once per launch and
-# writes each bitmap once, so its traffic grows in proportion).
+# DRAM traffic of a step from one ncu capture each (dram__bytes_read.sum +
+# dram__bytes_write.sum of every launch of one step) beside that step's
+# algorithmic bytes (columns read once, one bitmap written per query).  The
+# timed workload's step is credited with the same traffic-to-bytes ratio
+# (its launches read the columns and write the bitmaps in proportion) and
+# `traffic` is that per launch, like `achieved`.  The batched step is the
+# shared-position pre-pass and two 512-query passes: the pre-pass writes
+# 8 B per row and pass (16 B) that the passes read back, traffic above the
+# algorithmic bytes by design.
 NCU_TRAFFIC = {
-    "batched": {"kernel": "batch4_kernel<4,16>", "capture": "3e7 rows x 4 columns, 512 queries, one launch",
-                "bytes": 480.4e6 + 1863.3e6, "launch_bytes": 4 * 4 * 3e7 + 512 * 3e7 / 8},
-    "single": {"kernel": "scan_fused_kernel<1,1>", "capture": "1e8 rows x 1 column, one launch",
-               "bytes": 408.9e6, "launch_bytes": 4 * 1e8 + 1e8 / 8},
+    "batched": {"kernels": "pre_kernel<4,1> + 2 x batch4_kernel<4,16,16,true>",
+                "capture": "2e7 rows x 4 columns, 1024 queries: the three launches of one step",
+                "bytes": (320.09e6 + 275.12e6) + (160.21e6 + 1221.65e6) + (160.61e6 + 1223.99e6),
+                "step_bytes": 4 * 4 * 2e7 + 1024 * 2e7 / 8},
+    "single": {"kernels": "scan_fused_kernel<1,1>", "capture": "1e8 rows x 1 column, one launch",
+               "bytes": 408.9e6, "step_bytes": 4 * 1e8 + 1e8 / 8},
 }
 
 
-def launch_traffic(wl, n, queries, launches):
-    """Traffic of one launch of the timed workload scaled from its capture."""
+def step_traffic(wl, bytes_step, launches):
+    """Traffic of the timed workload's step scaled from its capture."""
     cap = NCU_TRAFFIC.get(wl)
     if cap is None:
         return None
-    used = {c for q in queries for c, _, _ in q}
-    own = 4 * n * len(used) + (len(queries) / launches) * n / 8
-    return {"bytes": round(cap["bytes"] / cap["launch_bytes"] * own / 1e9, 3), "unit": "GB",
-            "kernel": cap["kernel"], "capture": cap["capture"],
-            "launch_bytes_GB": round(own / 1e9, 3)}
+    t = cap["bytes"] / cap["step_bytes"] * bytes_step
+    return {"bytes": round(t / launches / 1e9, 3), "unit": "GB per launch", "GB_per_step": round(t / 1e9, 3),
+            "algorithmic_GB_per_step": round(bytes_step / 1e9, 3), "kernels": cap["kernels"],
+            "capture": cap["capture"]}
 
 
 def peaks():
@@ -469,7 +473,7 @@ def run(args):
     kern_launches = max(1, launches // args.steps)
     ms_launch = statistics.median(per) / kern_launches
     achieved = (bytes_step / kern_launches) / (ms_launch * 1e-3) / 1e9
-    tr = launch_traffic(wl, n, queries, kern_launches)
+    tr = step_traffic(wl, bytes_step, kern_launches)
 
     extra = {}
     if wl == "multi":
@@ -689,6 +693,33 @@ def event_median(torch, fn, reps=9, warm=3):
     return statistics.median(ts)
 
 
+def graph_per_call(torch, fn_on, calls=20, reps=7):
+    """Device time (ms) per call of fn_on(stream handle) with `calls` calls
+    captured in one CUDA graph (after the caller's warm-up calls) and the
+    graph replayed between two CUDA events: the calls' kernels back to back
+    without host work or launch gaps between them, median over `reps`."""
+    st = torch.cuda.current_stream()
+    cs = torch.cuda.Stream()
+    cs.wait_stream(st)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=cs):
+        for _ in range(calls):
+            fn_on(cs.cuda_stream)
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        g.replay()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / calls)
+    del g
+    return statistics.median(ts)
+
+
 def stream_per_call(torch, fn, calls=20, reps=5):
     """Device time (ms) per call of fn() issued `calls` times back to back
     between two CUDA events (host planning overlaps the device work, as in
@@ -785,9 +816,12 @@ def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
     quantiles) and columns of 256 and 64 distinct values (central value runs
     nearest those shares; the achieved selectivity is reported).  Times are
     the device time per query in a stream of 20 back-to-back calls (`_us`,
-    the basis of GB/s and frac) and the latency of one call alone
+    the basis of GB/s and frac), the latency of one call alone
     (`_latency_us`, which includes the host's planning and launch of that
-    call while the device waits).  Fused bytes: 4N + N/8.  BinDex bytes are those of the plan its planner picks,
+    call while the device waits), and for the BinDex the device time per
+    query of 20 calls replayed as one CUDA graph (`bindex_graph_us` and its
+    `bindex_graph_frac`: the query's kernels without the gaps between
+    launches from the host, which a stream of sub-20-us queries shows).  Fused bytes: 4N + N/8.  BinDex bytes are those of the plan its planner picks,
     from exact ranks, costed as bindex_query (csrc/bindex.cu) costs it: the
     result write, every filter vector read, and 12 B per re-tested row (its
     row id, its gathered value and its result word); a query whose matches
@@ -844,10 +878,12 @@ def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
             cand_cost = n / 8 + (match + 2048) * 40.0
             refine_only = cand_cost < sieve_cost
             nbytes = n / 8 + match * 12 if refine_only else n / 8 * (1 + fv_reads) + refine * 12
-            bq = lambda: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), s.cuda_stream)
+            bq_on = lambda st: c.bindex_scan_async(terms, bm.data_ptr(), cnt.data_ptr(), st)
+            bq = lambda: bq_on(s.cuda_stream)
             fq = lambda: c.scan_async(terms, ref.data_ptr(), cnt.data_ptr(), s.cuda_stream)
             lat_b = event_median(torch, bq, reps=7)
             t_b = stream_per_call(torch, bq)
+            g_b = graph_per_call(torch, bq_on)
             hits = int(cnt.item())
             lat_f = event_median(torch, fq, reps=7)
             t_f = stream_per_call(torch, fq)
@@ -862,6 +898,8 @@ def sweep_leg(torch, R, D, dev, n, hbm_peak, K=128):
                 "bindex_refined_rows": match if refine_only else refine, "bindex_bytes_MB": round(nbytes / 1e6, 2),
                 "bindex_GB_s": round(nbytes / (t_b * 1e-3) / 1e9, 1),
                 "bindex_frac": round(nbytes / (t_b * 1e-3) / 1e9 / hbm_peak, 4),
+                "bindex_graph_us": round(g_b * 1e3, 1),
+                "bindex_graph_frac": round(nbytes / (g_b * 1e-3) / 1e9 / hbm_peak, 4),
                 "equal": bool(torch.equal(bm, ref)) and hits == int(cnt.item())})
         res.setdefault("bindex_build_ms", {})[kind] = round(build_ms, 1)
         c.close()

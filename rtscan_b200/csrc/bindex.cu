@@ -161,13 +161,15 @@ void launch_fv(const uint32_t *col, uint64_t n, const uint32_t *start, int K, ui
 // ---- query -------------------------------------------------------------------
 //
 // A query is two launches on the caller's stream: the sieve kernel writes
-// every result word once (U & ~L over terms, or zeros in candidate mode)
-// while one warp of its first block per refine range resolves the range's
-// ends (warp searches in the sorted values, latency hidden behind the
-// streaming); its blocks sum their popcounts into a context slot and the
-// last block to finish (an arrival ticket, no waiting) stores the count.
-// The refine kernel then reads the resolved ranges from the slot, re-tests
-// their rows and corrects the bits and the count with atomics.
+// every result word once (U & ~L over terms, or zeros in candidate mode);
+// its blocks sum their popcounts into a context slot and the last block to
+// finish (an arrival ticket, no waiting) stores the count.  The refine
+// kernel, launched as a programmatic dependent of the sieve, resolves the
+// refine ranges' ends (warp searches in the sorted values) and tests its
+// first rows while the sieve streams, then corrects the rows whose bit the
+// sieve got wrong, and the count, with atomics.  Small refine sets are
+// re-tested by the sieve's last block instead (its block 0 resolves their
+// ends into the slot).
 
 // A refine range end: a known sorted rank, or the lower bound of `b` in the
 // sorted values, searched in [wlo, whi].
@@ -182,15 +184,26 @@ struct RefineRange {
   const uint32_t *sval;
   const uint32_t *spos;
   RangeEnd e0, e1;
-  int term;  // the term on this range's column (its value is sval[i])
+  int term;              // the term on this range's column (its value is sval[i])
+  uint32_t wlo, wspan;   // the values of its rows: x - wlo <= wspan (the ends' lower bounds)
+  int wok;               // 0: an empty range
+};
+
+// The sieve's verdict on one term of a row, as a value range: the filter
+// vectors it ANDs are (x < start) bits, so U & ~L holds exactly for
+// lo <= x < hi of the chosen areas' start values; ok = 0 when it holds for
+// no value.
+struct ApproxTerm {
+  uint32_t lo, span;
+  int ok;
 };
 
 }  // namespace
 
-// Context memory shared by the two launches of one query (kQuerySlots of
-// them, used in turn, so queries on different streams do not share one):
-// the resolved refine ranges, and the sieve's running count and finished
-// blocks, both zero between queries.
+// Context memory shared by the launches of one query (kQuerySlots of them,
+// used in turn, so queries on different streams do not share one): the
+// refine ranges the sieve's last block re-tests, and the sieve's running
+// count and finished blocks, both zero between queries.
 struct QuerySlot {
   unsigned long long acc;
   unsigned int ticket;
@@ -223,6 +236,7 @@ struct SieveParams {
   int refine_here;
   int zero_start;
   DevTerm rt[kFusedMaxTerms];
+  ApproxTerm ra[kFusedMaxTerms];
   int rnterms;
 };
 
@@ -246,51 +260,74 @@ __device__ uint64_t resolve_end(const RefineRange &rg, const RangeEnd &e) {
   return warp_lower_bound(rg.sval, e.wlo, e.whi, e.b);
 }
 
+// Wait for the grid this one depends on (launched with programmatic stream
+// serialization) to complete, its writes visible; returns at once in a grid
+// launched without it.
+__device__ __forceinline__ void wait_prerequisite() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Re-test the rows of the refine ranges (ends begin[r], end[r]) that fall to
-// thread `tid` of `stride`, set or clear their bits; returns the change of
-// the count.  Two rows per iteration: their loads (row id, own value,
-// gathers) are issued before either row's test and atomic.
-__device__ long long refine_rows(const RefineRange *ranges, int nranges, const DevTerm *terms, int nterms,
-                                 const unsigned long long *begin, const unsigned long long *end, uint64_t tid,
-                                 uint64_t stride, bool zero_start, uint32_t *out) {
+// thread `tid` of `stride`, correct their bits; returns the change of the
+// count.  A row's bit as the sieve left it is the AND of the terms'
+// ApproxTerm verdicts on its values (zero in candidate mode), its right bit
+// the AND of the exact terms, so only rows whose two differ are written,
+// with atomics whose old value is not needed.  A row in several ranges
+// (the windows of two terms) is corrected and counted by the first of them.
+// R rows per iteration: their loads (row id, own value, gathers) are
+// issued before any row's test.  kWait: the bits belong to the grid this
+// one depends on, so the first atomic waits for it (the loads and tests of
+// the first rows before it overlap that grid).
+template <bool kWait, int R>
+__device__ long long refine_rows(const RefineRange *ranges, int nranges, const DevTerm *terms,
+                                 const ApproxTerm *approx, int nterms, const unsigned long long *begin,
+                                 const unsigned long long *end, uint64_t tid, uint64_t stride, bool zero_start,
+                                 uint32_t *out) {
   long long delta = 0;
-  auto apply = [&](uint32_t row, bool hit) {
-    const uint32_t bit = 1u << (31 - (row & 31));
-    uint32_t *word = out + (row >> 5);
-    if (hit) {
-      const uint32_t old = atomicOr(word, bit);
-      delta += (old & bit) ? 0 : 1;
-    } else if (!zero_start) {  // in candidate mode the bit is still zero
-      const uint32_t old = atomicAnd(word, ~bit);
-      delta -= (old & bit) ? 1 : 0;
-    }
-  };
+  bool waited = !kWait;
   for (int r = 0; r < nranges; r++) {
     const RefineRange &rg = ranges[r];
     const uint64_t e = end[r];
-    for (uint64_t i = begin[r] + tid; i < e; i += 2 * stride) {
-      const uint64_t i2 = i + stride;
-      const bool two = i2 < e;
-      const uint32_t row = __ldg(rg.spos + i), own = __ldg(rg.sval + i);
-      const uint32_t row2 = two ? __ldg(rg.spos + i2) : row, own2 = two ? __ldg(rg.sval + i2) : own;
-      bool hit = true, hit2 = true;
-      for (int t = 0; t < nterms; t++) {
-        const bool mine = t == rg.term;
-        const uint32_t x = mine ? own : __ldg(terms[t].col + row);
-        const uint32_t x2 = mine ? own2 : __ldg(terms[t].col + row2);
-        hit = hit && x - terms[t].lo <= terms[t].span;
-        hit2 = hit2 && x2 - terms[t].lo <= terms[t].span;
+    for (uint64_t i = begin[r] + tid; i < e; i += R * stride) {
+      uint32_t row[R];
+      int flip[R];  // +1 set, -1 clear, 0 leave
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+        const uint64_t ik = i + k * stride;
+        const bool in = ik < e;
+        row[k] = in ? __ldg(rg.spos + ik) : 0u;
+        const uint32_t own = in ? __ldg(rg.sval + ik) : 0u;
+        bool now = true, was = !zero_start, first = in;
+        for (int t = 0; t < nterms; t++) {
+          const uint32_t x = t == rg.term ? own : __ldg(terms[t].col + row[k]);
+          now = now && x - terms[t].lo <= terms[t].span;
+          was = was && approx[t].ok && x - approx[t].lo <= approx[t].span;
+          for (int q = 0; q < r; q++)
+            first = first && !(ranges[q].term == t && ranges[q].wok && x - ranges[q].wlo <= ranges[q].wspan);
+        }
+        flip[k] = first ? (int)now - (int)was : 0;
       }
-      apply(row, hit);
-      if (two) apply(row2, hit2);
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+        if (!flip[k]) continue;
+        if (!waited) {
+          wait_prerequisite();
+          waited = true;
+        }
+        const uint32_t bit = 1u << (31 - (row[k] & 31));
+        uint32_t *word = out + (row[k] >> 5);
+        if (flip[k] > 0) atomicOr(word, bit);
+        else atomicAnd(word, ~bit);
+        delta += flip[k];
+      }
     }
   }
   return delta;
 }
 
 __global__ void __launch_bounds__(kThreads) sieve_kernel(const __grid_constant__ SieveParams p) {
+  // a refine grid launched after this one may start now (see refine_kernel)
+  asm volatile("griddepcontrol.launch_dependents;");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (blockIdx.x == 0) {
+  if (p.refine_here && blockIdx.x == 0) {
     for (int r = warp; r < p.nranges; r += kThreads / 32) {
       const uint64_t a = resolve_end(p.r[r], p.r[r].e0);
       const uint64_t b = resolve_end(p.r[r], p.r[r].e1);
@@ -369,8 +406,8 @@ __global__ void __launch_bounds__(kThreads) sieve_kernel(const __grid_constant__
       s_end[r] = p.slot->end[r];
     }
     __syncthreads();
-    delta = refine_rows(p.r, p.nranges, p.rt, p.rnterms, s_begin, s_end, threadIdx.x, kThreads, p.zero_start != 0,
-                        p.out);
+    delta = refine_rows<false, 2>(p.r, p.nranges, p.rt, p.ra, p.rnterms, s_begin, s_end, threadIdx.x, kThreads,
+                                  p.zero_start != 0, p.out);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) delta += __shfl_xor_sync(kFull, delta, o);
@@ -387,34 +424,46 @@ __global__ void __launch_bounds__(kThreads) sieve_kernel(const __grid_constant__
 
 struct RefineParams {
   DevTerm t[kFusedMaxTerms];
+  ApproxTerm a[kFusedMaxTerms];
   int nterms;
   RefineRange r[kMaxBounds];
   int nranges;
-  const QuerySlot *slot;  // the ranges' resolved ends
   int zero_start;         // candidate mode: every bit starts at zero, so misses write nothing
   uint32_t *out;
   unsigned long long *count;
 };
 
+constexpr int kRefineRows = 2;  // rows per thread and iteration of refine_kernel
+
+// Launched right behind the sieve (or the zero fill of a candidate plan)
+// with programmatic stream serialization, so that its first blocks run
+// beside that grid: every block resolves the ranges' ends itself (binary
+// searches in the sorted values) and loads and tests its first rows, and
+// waits for the bitmap only before its first atomic.
 __global__ void __launch_bounds__(kThreads) refine_kernel(const __grid_constant__ RefineParams p) {
   __shared__ unsigned long long s_begin[kMaxBounds], s_end[kMaxBounds];
   __shared__ long long part[kThreads / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r = threadIdx.x; r < p.nranges; r += kThreads) {
-    s_begin[r] = p.slot->begin[r];
-    s_end[r] = p.slot->end[r];
+  for (int r = warp; r < p.nranges; r += kThreads / 32) {
+    const uint64_t a = resolve_end(p.r[r], p.r[r].e0);
+    const uint64_t b = resolve_end(p.r[r], p.r[r].e1);
+    if (lane == 0) {
+      s_begin[r] = min(a, b);
+      s_end[r] = max(a, b);
+    }
   }
   __syncthreads();
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  const long long delta =
-      refine_rows(p.r, p.nranges, p.t, p.nterms, s_begin, s_end, tid, stride, p.zero_start != 0, p.out);
+  const long long delta = refine_rows<true, kRefineRows>(p.r, p.nranges, p.t, p.a, p.nterms, s_begin, s_end, tid,
+                                                         stride, p.zero_start != 0, p.out);
   long long d = delta;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
   if (lane == 0) part[warp] = d;
   __syncthreads();
   if (threadIdx.x == 0) {
+    wait_prerequisite();  // the count is the sieve's until then (also for a block without rows)
     long long s = 0;
     for (int i = 0; i < kThreads / 32; i++) s += part[i];
     if (s) atomicAdd(p.count, (unsigned long long)s);
@@ -686,6 +735,18 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
   const uint32_t rem = (uint32_t)(n & 31);
   sp.tail_mask = rem ? ~(0xFFFFFFFFu >> rem) : 0xFFFFFFFFu;
   sp.vec = ((uintptr_t)out & 15) == 0;
+  // The value an approximation stands for: fv[k] holds x < start[k+1];
+  // k = -1 is no row (x < 0), k = K-1 every row (x < 2^32).
+  auto approx_value = [&](const GpuBinDex &B, const Approx &a) -> uint64_t {
+    return a.k < 0 ? 0 : a.k >= B.K - 1 ? (1ull << 32) : B.start[a.k + 1];
+  };
+  // A range's rows are those whose value lies between its ends' bounds.
+  auto window = [](RefineRange &rg, uint64_t v0, uint64_t v1) {
+    const uint64_t a = std::min(v0, v1), b = std::max(v0, v1);
+    rg.wok = a < b;
+    rg.wlo = (uint32_t)a;
+    rg.wspan = a < b ? (uint32_t)(b - 1 - a) : 0u;
+  };
   if (best_cand_cost < sieve_cost) {
     // Candidate mode: start from zero, re-test the matches of one term.
     const int t = best_cand;
@@ -696,6 +757,7 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
     rg.term = t;
     rg.e0 = tp[t].has_lo ? end_of(tp[t].e_lo, tlo[t]) : end_rank(0);
     rg.e1 = tp[t].has_hi ? end_of(tp[t].e_hi, thi[t] + 1) : end_rank(n);
+    window(rg, tp[t].has_lo ? tlo[t] : 0, tp[t].has_hi ? (uint64_t)thi[t] + 1 : (1ull << 32));
     rp.nranges = 1;
     rp.zero_start = 1;
   } else {
@@ -710,6 +772,12 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
       if (!tp[t].has_lo || tp[t].a_lo.k < 0) { st.L = nullptr; st.l_const = 0u; }
       else if (tp[t].a_lo.k == B.K - 1) { st.L = nullptr; st.l_const = ~0u; }
       else st.L = B.fv + (uint64_t)tp[t].a_lo.k * B.fv_stride;
+      // the same verdict as a value range: lb <= x < ub
+      const uint64_t ub = tp[t].has_hi ? approx_value(B, tp[t].a_hi) : (1ull << 32);
+      const uint64_t lb = tp[t].has_lo ? approx_value(B, tp[t].a_lo) : 0;
+      rp.a[t].ok = lb < ub;
+      rp.a[t].lo = (uint32_t)lb;
+      rp.a[t].span = lb < ub ? (uint32_t)(ub - 1 - lb) : 0u;
       if (tp[t].has_hi) {
         RefineRange &rg = rp.r[rp.nranges++];
         rg.sval = B.sval;
@@ -717,6 +785,7 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
         rg.term = t;
         rg.e0 = end_of(tp[t].e_hi, thi[t] + 1);
         rg.e1 = end_rank(tp[t].a_hi.rank);
+        window(rg, (uint64_t)thi[t] + 1, approx_value(B, tp[t].a_hi));
       }
       if (tp[t].has_lo) {
         RefineRange &rg = rp.r[rp.nranges++];
@@ -725,6 +794,7 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
         rg.term = t;
         rg.e0 = end_of(tp[t].e_lo, tlo[t]);
         rg.e1 = end_rank(tp[t].a_lo.rank);
+        window(rg, tlo[t], approx_value(B, tp[t].a_lo));
       }
     }
   }
@@ -749,15 +819,26 @@ void bindex_query(rts_ctx *ctx, const rts_term *terms, int nterms, uint32_t *out
     sp.refine_here = 1;
     sp.zero_start = rp.zero_start;
     sp.rnterms = rp.nterms;
-    for (int t = 0; t < rp.nterms; t++) sp.rt[t] = rp.t[t];
+    for (int t = 0; t < rp.nterms; t++) {
+      sp.rt[t] = rp.t[t];
+      sp.ra[t] = rp.a[t];
+    }
   }
   const uint64_t nvec = sp.words / 4 + 1;
   sieve_kernel<<<blocks_for(nvec, ctx->sm_count, 4), kThreads, 0, s>>>(sp);  // one wave: 48 registers allow 5 blocks per SM
   launches++;
   if (rp.nranges && !sp.refine_here) {
-    rp.slot = slot;
-    const uint64_t refine_rows = est_rows;
-    refine_kernel<<<blocks_for(std::max<uint64_t>(refine_rows, 1), ctx->sm_count, 8), kThreads, 0, s>>>(rp);
+    cudaLaunchConfig_t cfg = {};
+    const uint64_t threads = (std::max<uint64_t>(est_rows, 1) + kRefineRows - 1) / kRefineRows;
+    cfg.gridDim = dim3(blocks_for(threads, ctx->sm_count, 8));
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    RTS_CUDA(cudaLaunchKernelEx(&cfg, refine_kernel, rp));
     launches++;
   }
   RTS_CUDA(cudaGetLastError());

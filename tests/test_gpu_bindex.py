@@ -86,6 +86,36 @@ def test_conjunctive_queries(ctx, ncols):
         assert np.array_equal(got, want), q
 
 
+def test_rows_in_two_refine_ranges(ctx):
+    """Rows that lie in the refine windows of two terms (identical columns
+    with equal or overlapping bounds, both bounds of a term inside one area)
+    are corrected and counted once; refine sets of thousands of rows take
+    the refine launch, small ones the sieve's last block."""
+    n = (1 << 21) + 7
+    a = D.uniform(n, 91)
+    b = a.copy()
+    c = (a ^ np.uint32(0x5A5A)).astype(np.uint32)
+    cols = [a, b, c]
+    ctx.load_columns(cols)
+    for i in range(3):
+        ctx.build_bindex(i, 128)
+    s = np.sort(a)
+    rng = np.random.default_rng(5)
+    qs = []
+    for _ in range(12):
+        i, j = sorted(rng.integers(0, n, size=2).tolist())
+        lo, hi = int(s[i]), int(s[j])
+        qs.append([(0, lo, hi), (1, lo, hi)])
+        k = int(rng.integers(0, n - 20000))
+        qs.append([(0, int(s[k]), int(s[k + 9000])), (1, int(s[k + 3000]), int(s[k + 15000]))])
+        qs.append([(0, int(s[k]), int(s[k + 500])), (1, int(s[k + 100]), int(s[k + 700])), (2, 0, 0xFFFF0000)])
+    for q in qs:
+        got, cnt = bindex_scan(ctx, q)
+        want, wcnt = expect(cols, q)
+        assert cnt == wcnt, (q, cnt, wcnt)
+        assert np.array_equal(got, want), q
+
+
 def test_missing_index_is_an_error(ctx):
     n = 10_000
     ctx.load_columns([D.uniform(n, 1), D.uniform(n, 2)])
