@@ -547,8 +547,10 @@ def run(args):
         if world > 1:
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
         e2e_s = float(et.item())
+        h2d_b, d2h_b = ctx.host_transfer_bytes()
         e2e = {"value": round(bytes_step * world / e2e_s / 1e9, 3), "unit": "GB/s",
-               "h2d_bytes_per_step": int(4 * n * len(cols)), "d2h_bytes_per_step": int(nq * (stride * 4 + 8)),
+               "h2d_bytes_per_step": int(h2d_b), "d2h_bytes_per_step": int(d2h_b),
+               "dense_d2h_bytes_per_step": int(nq * (R.bitmap_words(n) * 4 + 8)),
                "queries_per_s": round(nq * world / e2e_s, 2), "ms_per_step": round(e2e_s * 1e3, 2),
                "calls_ms": [round(c * 1e3, 1) for c in calls], "timing": "median of 5 calls after one warm-up",
                "api": "rts_scan_batch_host"}

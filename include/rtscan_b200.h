@@ -231,15 +231,21 @@ RTS_API rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, con
                                         uint64_t *dev_counts, void *stream);
 /* Batched scan over host-resident columns into host bitmaps: uploads the
  * `ncols` columns of `nrows` values (pinned host memory is fastest), runs
- * the batched passes, and copies every query's bitmap (host_bitmaps +
- * q*stride_words) and count (host_counts[q]) back, the download of each
- * group of queries overlapping the next group's pass.  Blocking.  The
+ * the batched passes, and writes every query's bitmap (host_bitmaps +
+ * q*stride_words) and count (host_counts[q]), the download of each row
+ * chunk overlapping the next chunk's pass (sparse chunks of a bitmap are
+ * sent as pairs and expanded by host threads).  Blocking.  The
  * context's resident table is left as it was.  (The reference's per-query
  * upload-scan-download loop, bindex_cuda.cpp:1771-1946.) */
 RTS_API rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
                                        uint64_t nrows, const rts_term *terms, const int32_t *offsets,
                                        int32_t nqueries, uint32_t *host_bitmaps, uint64_t stride_words,
                                        uint64_t *host_counts);
+/* Bytes the context's last rts_scan_batch_host call moved host to device
+ * (columns, plan) and device to host (bitmaps: a query whose row chunk has
+ * at most one nonzero word in eight travels as (word, value) pairs that the
+ * call expands into host_bitmaps; counts).  Zero before the first call. */
+RTS_API rts_status rts_host_transfer_bytes(const rts_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* The same queries with one fused-scan launch per query (the baseline the
  * batched kernel is measured against). */
 RTS_API rts_status rts_scan_each_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets,

@@ -116,6 +116,7 @@ _SIGS = [
     ("rts_scan_batch_host", ctypes.c_int32, [_P, ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64, _TERMP,
                                              ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P, ctypes.c_uint64,
                                              _P]),
+    ("rts_host_transfer_bytes", ctypes.c_int32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("rts_scan_separate_noalloc_async", ctypes.c_int32, [ctypes.POINTER(_P), ctypes.c_int32, ctypes.c_uint64,
                                                          _TERMP, ctypes.c_int32, _P, _P, _P]),
     ("rts_encode_table", ctypes.c_int32, [_P, ctypes.c_uint32, ctypes.c_uint32]),
@@ -527,6 +528,12 @@ class Context:
         self._c(lib().rts_scan_batch_host(self._h, ptrs, len(host_cols), n, arr, off, len(queries),
                                           host_bitmaps.ctypes.data, stride, counts.ctypes.data))
         return host_bitmaps, counts
+
+    def host_transfer_bytes(self):
+        """(host-to-device, device-to-host) bytes of the last scan_batch_host."""
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self._c(lib().rts_host_transfer_bytes(self._h, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return int(h2d.value), int(d2h.value)
 
     def prepare_batch(self, queries, bitmaps_ptr: int, stride_words: int, counts_ptr: int) -> "PreparedBatch":
         """Plan `queries` once and capture their launches in a CUDA graph."""

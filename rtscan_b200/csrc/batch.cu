@@ -29,8 +29,13 @@
 // fused scan), so the result of every query equals the single-query path.
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -511,6 +516,7 @@ void launch_one(const BatchPass &bp, int sm_count, cudaStream_t s) {
 
 #include "batch4.cuh"
 #include "batch_few.cuh"
+#include "sparse_d2h.cuh"
 
 template <int CMAX, int GV, int W>
 size_t smem_bytes4(uint32_t blob_words) {
@@ -803,45 +809,48 @@ int launch_outside(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::
 std::vector<uint16_t> bucket_index(const std::vector<uint32_t> &B, uint64_t span, uint32_t nb_target,
                                    uint32_t *shift_out, uint32_t *lgm_out) {
   const uint32_t m = (uint32_t)B.size(), bmin = B.front();
-  auto depth = [&](const std::vector<uint16_t> &bk, auto &&bucket) {
+  // Search depth of the boundaries (all but the last) under a bucket map:
+  // the sorted boundaries fall into non-decreasing buckets, so each run of
+  // equal buckets is one bucket's boundaries (no index is built).
+  auto depth = [&](auto &&bucket) {
     double d = 0;
-    for (uint32_t i = 0; i + 1 < m; i++) {
-      const uint32_t k = bucket(B[i] - bmin);
-      uint32_t n = (uint32_t)(bk[k + 1] - bk[k]), it = 0;
-      while (n) { it++; n >>= 1; }
-      d += it;
+    for (uint32_t lo = 0; lo < m;) {
+      const uint32_t k = bucket(B[lo] - bmin);
+      uint32_t hi = lo + 1;
+      while (hi < m && bucket(B[hi] - bmin) == k) hi++;
+      uint32_t it = 0;
+      for (uint32_t n = hi - lo; n; n >>= 1) it++;
+      d += (double)it * (hi - lo - (hi == m ? 1 : 0));
+      lo = hi;
     }
     return d;
+  };
+  // the index of a bucket map over nb buckets: first boundary whose bucket is >= k
+  auto index = [&](uint32_t nb, auto &&bucket) {
+    std::vector<uint16_t> bk(nb + 1);
+    uint32_t i = 0;
+    for (uint32_t k = 0; k <= nb; k++) {
+      while (i < m && bucket(B[i] - bmin) < k) i++;
+      bk[k] = (uint16_t)i;
+    }
+    return bk;
   };
   uint32_t shift = 0;
   while ((span >> shift) > nb_target) shift++;
   const uint32_t nb = (uint32_t)(((span - 1) >> shift) + 1);  // buckets covering [bmin, bmax]
-  std::vector<uint16_t> lin(nb + 1);
-  uint32_t j = 0;
-  for (uint32_t k = 0; k <= nb; k++) {  // first boundary at or above the bucket's start
-    const uint64_t start = (uint64_t)bmin + ((uint64_t)k << shift);
-    while (j < m && (uint64_t)B[j] < start) j++;
-    lin[k] = (uint16_t)j;
-  }
+  auto lin = [&](uint32_t v) { return v >> shift; };
   *shift_out = shift;
   *lgm_out = 0;
   uint32_t M = 12;
   while (M > 0 && bucket_of((uint32_t)(span - 1), M) + 1 > nb_target) M--;
-  if (M == 0) return lin;
-  const uint32_t nbl = bucket_of((uint32_t)(span - 1), M) + 1;
-  std::vector<uint16_t> lg(nbl + 1, 0);
-  uint32_t i = 0;
-  for (uint32_t k = 0; k <= nbl; k++) {  // first boundary whose bucket is >= k
-    while (i < m && bucket_of(B[i] - bmin, M) < k) i++;
-    lg[k] = (uint16_t)i;
+  if (M > 0) {
+    auto lg = [&](uint32_t v) { return bucket_of(v, M); };
+    if (depth(lg) < depth(lin)) {
+      *lgm_out = M;
+      return index(bucket_of((uint32_t)(span - 1), M) + 1, lg);
+    }
   }
-  const double dl = depth(lin, [&](uint32_t v) { return v >> shift; });
-  const double dg = depth(lg, [&](uint32_t v) { return bucket_of(v, M); });
-  if (dg < dl) {
-    *lgm_out = M;
-    return lg;
-  }
-  return lin;
+  return index(nb, lin);
 }
 
 bool runs_in_kernel(const NormQuery &q) { return !q.empty && !q.cols.empty() && (int)q.cols.size() <= kMaxCols; }
@@ -873,38 +882,38 @@ std::vector<uint32_t> pre_buckets(const std::vector<uint32_t> &B, PreCol &pc) {
     pc.nbk = 1;
     return {0u};
   }
-  auto entries = [&](uint32_t M, uint32_t L, uint32_t nbk, double *cost) {
+  // Search steps of every boundary under bucket shape (M, L): the sorted
+  // boundaries fall into non-decreasing buckets, so each run of equal
+  // buckets is one bucket's boundaries (no index is built).
+  auto cost_of = [&](uint32_t M, uint32_t L, uint32_t nbk) {
     PreCol t = pc;
     t.M = M;
     t.L = L;
     t.nbk = nbk;
-    std::vector<uint32_t> ent(nbk);
-    std::vector<uint32_t> first(nbk + 1, m);  // first boundary whose bucket is >= k
-    for (uint32_t i = m; i-- > 0;) first[pre_bucket(t, B[i])] = i;
-    for (uint32_t k = nbk; k-- > 0;) first[k] = std::min(first[k], first[k + 1]);
-    *cost = 0;
-    for (uint32_t k = 0; k < nbk; k++) {
-      const uint32_t lo = first[k], hi = k + 1 < nbk ? first[k + 1] : m;
+    double cost = 0;
+    for (uint32_t lo = 0; lo < m;) {
+      const uint32_t k = pre_bucket(t, B[lo]);
+      uint32_t hi = lo + 1;
+      while (hi < m && pre_bucket(t, B[hi]) == k) hi++;
       const uint64_t start = (uint64_t)pc.origin + pre_bucket_start(M, L, k);
-      const uint32_t base = lo + (lo < hi && B[lo] == start ? 1u : 0u);
-      const uint32_t n = hi - base;
-      ent[k] = base | n << 16;
+      const uint32_t n = hi - lo - (B[lo] == start ? 1u : 0u);
       uint32_t steps = 0;
       for (uint32_t r = n; r; r >>= 1) steps++;
-      *cost += (double)steps * (hi - lo);
+      cost += (double)steps * (hi - lo);
+      lo = hi;
     }
-    return ent;
+    return cost;
   };
   const uint32_t vmax = B.back() - pc.origin;
-  struct Cand {
-    uint32_t M, L, nbk;
-  };
-  std::vector<Cand> cands;
+  uint32_t bestM, bestL, bestN;
   {
     uint32_t L = 0;
     while ((vmax >> L) >= kPreMaxBuckets) L++;
-    cands.push_back({31, L, (vmax >> L) + 1});
+    bestM = 31;
+    bestL = L;
+    bestN = (vmax >> L) + 1;
   }
+  double best_cost = cost_of(bestM, bestL, bestN);
   for (uint32_t M = 1; M <= 12; M++)
     for (uint32_t L = 0; L < 32; L++) {
       PreCol t = pc;
@@ -912,25 +921,31 @@ std::vector<uint32_t> pre_buckets(const std::vector<uint32_t> &B, PreCol &pc) {
       t.L = L;
       t.nbk = 0xFFFFFFFFu;
       const uint32_t nbk = pre_bucket(t, B.back()) + 1;
-      if (nbk <= kPreMaxBuckets) {
-        cands.push_back({M, L, nbk});
-        break;
+      if (nbk > kPreMaxBuckets) continue;
+      const double cost = cost_of(M, L, nbk);
+      if (cost < best_cost || (cost == best_cost && nbk < bestN)) {
+        best_cost = cost;
+        bestM = M;
+        bestL = L;
+        bestN = nbk;
       }
+      break;
     }
-  std::vector<uint32_t> best;
-  double best_cost = 0;
-  for (const Cand &cd : cands) {
-    double cost;
-    std::vector<uint32_t> ent = entries(cd.M, cd.L, cd.nbk, &cost);
-    if (best.empty() || cost < best_cost || (cost == best_cost && ent.size() < best.size())) {
-      best = std::move(ent);
-      best_cost = cost;
-      pc.M = cd.M;
-      pc.L = cd.L;
-      pc.nbk = cd.nbk;
-    }
+  pc.M = bestM;
+  pc.L = bestL;
+  pc.nbk = bestN;
+  // the index: entry k = base | n << 16 (see PreCol)
+  std::vector<uint32_t> ent(bestN);
+  uint32_t lo = 0;
+  for (uint32_t k = 0; k < bestN; k++) {
+    uint32_t hi = lo;
+    while (hi < m && (k + 1 == bestN || pre_bucket(pc, B[hi]) == k)) hi++;
+    const uint64_t start = (uint64_t)pc.origin + pre_bucket_start(bestM, bestL, k);
+    const uint32_t base = lo + (lo < hi && B[lo] == start ? 1u : 0u);
+    ent[k] = base | (hi - base) << 16;
+    lo = hi;
   }
-  return best;
+  return ent;
 }
 
 // Move column s of `src` to column c of `dst` (a pass's per-column fields).
@@ -1096,11 +1111,13 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
     // tables: row pos holds, per slot, whether the values of interval pos
     // ([B[pos-1], B[pos]) with B[-1] = 0, B[m] = 2^32) pass the slot's term
     // on this column (always, when the slot does not constrain it).  Built
-    // as XOR deltas at the interval ends and a prefix XOR over positions;
-    // a term [lo, hi] covers positions pos(lo) .. pos(hi) with pos(x) =
-    // #{B <= x}, where lo and hi + 1 are themselves boundaries.
-    std::vector<std::vector<uint32_t>> delta(C);
-    for (int c = 0; c < C; c++) delta[c].assign((size_t)(bp.m[c] + 2) * Gp, 0u);
+    // in place as XOR deltas at the interval ends and a prefix XOR over
+    // positions; a term [lo, hi] covers positions pos(lo) .. pos(hi) with
+    // pos(x) = #{B <= x}, where lo and hi + 1 are themselves boundaries.
+    for (int c = 0; c < C; c++) {
+      bp.tab_off[c] = (uint32_t)blob.size();
+      blob.resize(blob.size() + (size_t)(bp.m[c] + 1) * Gp, 0u);
+    }
     std::vector<uint32_t> free_mask((size_t)C * Gp, 0u);  // slots leaving column c unconstrained
     for (int slot = 0; slot < (int)pp.qs.size(); slot++) {
       const uint32_t bit = 1u << (slot & 31);
@@ -1116,23 +1133,16 @@ BatchPlan build_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std
         const uint32_t p1 = q.hi[k] < 0xFFFFFFFFu
                                 ? (uint32_t)(std::lower_bound(Bc.begin(), Bc.end(), q.hi[k] + 1) - Bc.begin())
                                 : m;
-        delta[c][(size_t)p0 * Gp + grp] ^= bit;
-        delta[c][(size_t)(p1 + 1) * Gp + grp] ^= bit;
+        uint32_t *tab = blob.data() + bp.tab_off[c];
+        tab[(size_t)p0 * Gp + grp] ^= bit;
+        if (p1 + 1 <= m) tab[(size_t)(p1 + 1) * Gp + grp] ^= bit;
         free_mask[(size_t)c * Gp + grp] &= ~bit;
       }
     }
     for (int c = 0; c < C; c++) {
-      const uint32_t m = bp.m[c];
-      for (int grp = 0; grp < Gp; grp++) {  // unconstrained slots pass every position
-        delta[c][grp] ^= free_mask[(size_t)c * Gp + grp];
-        delta[c][(size_t)(m + 1) * Gp + grp] ^= free_mask[(size_t)c * Gp + grp];
-      }
-      bp.tab_off[c] = (uint32_t)blob.size();
-      blob.resize(blob.size() + (size_t)(m + 1) * Gp, 0u);
       uint32_t *tab = blob.data() + bp.tab_off[c];
-      uint32_t acc[32] = {0};
-      for (uint32_t pos = 0; pos <= m; pos++)
-        for (int grp = 0; grp < Gp; grp++) tab[(size_t)pos * Gp + grp] = acc[grp] ^= delta[c][(size_t)pos * Gp + grp];
+      for (int grp = 0; grp < Gp; grp++) tab[grp] ^= free_mask[(size_t)c * Gp + grp];  // pass every position
+      for (size_t i = Gp; i < (size_t)(bp.m[c] + 1) * Gp; i++) tab[i] ^= tab[i - Gp];
     }
     // boundaries and bucket index.  The table budget counts 4 buckets per
     // boundary; a pass takes 16 where its shared memory still holds them:
@@ -1488,10 +1498,44 @@ struct HostBatchBuffers {
   size_t cnt_cap = 0;
   cudaStream_t up = nullptr, compute = nullptr, copy = nullptr;
   std::vector<cudaEvent_t> ev;
+  // sparse transfer: per chunk the queries' nonzero-word counts (device,
+  // pinned host), the packed queries and their pair offsets (pinned host,
+  // device), and the pairs (two device slots, three pinned host slots)
+  uint32_t *nnz = nullptr;
+  size_t nnz_cap = 0;
+  uint32_t *nnz_host = nullptr;
+  size_t nnz_host_cap = 0;
+  int32_t *ql = nullptr;
+  size_t ql_cap = 0;
+  uint64_t *qoff = nullptr;
+  size_t qoff_cap = 0;
+  int32_t *ql_host = nullptr;
+  size_t ql_host_cap = 0;
+  uint64_t *qoff_host = nullptr;
+  size_t qoff_host_cap = 0;
+  uint2 *pairs[2] = {nullptr, nullptr};
+  size_t pairs_cap[2] = {0, 0};
+  uint2 *pairs_host[3] = {nullptr, nullptr, nullptr};
+  size_t pairs_host_cap[3] = {0, 0, 0};
+  // bytes the last call moved each way
+  uint64_t last_h2d = 0, last_d2h = 0;
   ~HostBatchBuffers() {
+    if (up) cudaStreamSynchronize(up);
+    if (compute) cudaStreamSynchronize(compute);
+    if (copy) cudaStreamSynchronize(copy);
     if (cols) cudaFree(cols);
     if (bitmaps) cudaFree(bitmaps);
     if (counts) cudaFree(counts);
+    if (nnz) cudaFree(nnz);
+    if (ql) cudaFree(ql);
+    if (qoff) cudaFree(qoff);
+    for (auto *pp : pairs)
+      if (pp) cudaFree(pp);
+    if (nnz_host) cudaFreeHost(nnz_host);
+    if (ql_host) cudaFreeHost(ql_host);
+    if (qoff_host) cudaFreeHost(qoff_host);
+    for (auto *pp : pairs_host)
+      if (pp) cudaFreeHost(pp);
     for (auto e : ev) cudaEventDestroy(e);
     if (up) cudaStreamDestroy(up);
     if (compute) cudaStreamDestroy(compute);
@@ -1499,6 +1543,20 @@ struct HostBatchBuffers {
   }
 };
 void destroy_host_batch(HostBatchBuffers *b) { delete b; }
+
+// Pinned host memory of at least `count` elements (grown, contents dropped).
+template <class T>
+static void ensure_host(T *&p, size_t &cap, size_t count) {
+  if (cap >= count) return;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  if (cudaHostAlloc(reinterpret_cast<void **>(&p), std::max<size_t>(count, 1) * sizeof(T), 0) != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(RTS_ERR_NOMEM, "pinned host allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
+  }
+  cap = count;
+}
 
 template <class T>
 static void ensure(T *&p, size_t &cap, size_t count) {
@@ -1571,15 +1629,22 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     const uint64_t want_chunks = std::max<uint64_t>(1, std::min<uint64_t>(32, nrows >> 22));
     const uint64_t chunk_rows = ((nrows + want_chunks - 1) / want_chunks + 4095) / 4096 * 4096;
     const int nchunks = (int)((nrows + chunk_rows - 1) / chunk_rows);
-    while ((int)H.ev.size() < 2 * nchunks + 1) {
+    // events per chunk: upload, scan, counts on the host, pack, pairs on the host
+    const int kEv = 5;
+    while ((int)H.ev.size() < kEv * nchunks + 1) {
       cudaEvent_t e;
       RTS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       H.ev.push_back(e);
     }
+    auto ev = [&](int r, int k) { return H.ev[kEv * r + k]; };
     std::vector<rts::NormQuery> norm = rts::normalize_all(ctx, terms, offsets, nq);
     std::vector<int> inside, outside;
     for (int q = 0; q < nq; q++) (rts::runs_in_kernel(norm[q]) ? inside : outside).push_back(q);
+    std::vector<char> is_outside(std::max(nq, 1), 0);
+    for (int q : outside) is_outside[q] = 1;
     if (nq > 0) RTS_CUDA(cudaMemsetAsync(H.counts, 0, (size_t)nq * 8, H.compute));
+    H.last_h2d = (uint64_t)nrows * 4 * ncols;  // and below: the plan, the packed-query lists
+    H.last_d2h = (uint64_t)nq * 8;             // and below: bitmaps, pairs, nonzero-word counts
     rts::BatchPlan plan;
     const uint32_t *dev_blob = nullptr;
     cudaEvent_t blob_done = nullptr;
@@ -1588,47 +1653,156 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     if (!inside.empty()) {
       plan = rts::build_plan(ctx, norm, inside, nullptr, ctx->batch_cfg.table_budget, true);
       dev_blob = rts::upload_plan(ctx, plan, H.compute, &blob_done);
+      H.last_h2d += plan.blob.size() * 4;
       pre_bytes = rts::plan_pre_bytes(plan, chunk_rows);
       pre = rts::context_pre_scratch(ctx, pre_bytes, H.compute);
     }
+    // Sparse transfer (sparse_d2h.cuh) when a chunk holds enough words per
+    // query; a packed query has at most cw / 8 nonzero words in the chunk.
+    const uint64_t cw_max = chunk_rows / 32;
+    const bool sparse = nq > 0 && !inside.empty() && cw_max >= rts::kSparseMinWords;
+    const uint64_t max_pairs = sparse ? (uint64_t)nq * (cw_max / 8) : 0;
+    if (sparse) {
+      rts::ensure(H.nnz, H.nnz_cap, (size_t)nq * nchunks);
+      rts::ensure_host(H.nnz_host, H.nnz_host_cap, (size_t)nq * nchunks);
+      rts::ensure(H.ql, H.ql_cap, (size_t)nq * nchunks);
+      rts::ensure(H.qoff, H.qoff_cap, (size_t)nq * nchunks);
+      rts::ensure_host(H.ql_host, H.ql_host_cap, (size_t)nq * nchunks);
+      rts::ensure_host(H.qoff_host, H.qoff_host_cap, (size_t)nq * nchunks);
+      for (int i = 0; i < 2; i++) rts::ensure(H.pairs[i], H.pairs_cap[i], (size_t)max_pairs);
+      for (int i = 0; i < 3; i++) rts::ensure_host(H.pairs_host[i], H.pairs_host_cap[i], (size_t)max_pairs);
+    }
+    // Host threads that expand packed queries (declared after the buffers'
+    // owner, so that they are joined on every way out before the streams
+    // are drained; they only wait for events already recorded).
+    rts::SlotGate gate;
+    std::unique_ptr<rts::TaskPool> pool;
+    if (sparse) {
+      const unsigned hw = std::thread::hardware_concurrency();
+      pool.reset(new rts::TaskPool((int)std::max(1u, std::min(8u, hw ? hw / 2 : 4u))));
+    }
+    // Finish chunk r once its counts are on the host: the dense queries'
+    // words leave as one 2D copy per run of consecutive dense queries, the
+    // packed ones as pairs expanded by the pool.
+    auto finish = [&](int r) {
+      const uint64_t r0 = (uint64_t)r * chunk_rows, r1 = std::min<uint64_t>(nrows, r0 + chunk_rows);
+      const uint64_t w0 = r0 / 32, w1 = r1 == nrows ? words : r1 / 32, cw = w1 - w0;
+      std::vector<int> packed;
+      uint64_t total = 0;
+      const bool try_pack = sparse && cw >= rts::kSparseMinWords;
+      if (try_pack) RTS_CUDA(cudaEventSynchronize(ev(r, 2)));
+      int32_t *qlh = H.ql_host + (size_t)nq * r;
+      uint64_t *qoh = H.qoff_host + (size_t)nq * r;
+      int q = 0;
+      while (q < nq) {
+        if (is_outside[q]) {
+          q++;
+          continue;
+        }
+        const uint32_t c = try_pack ? H.nnz_host[(size_t)nq * r + q] : 0u;
+        if (try_pack && (uint64_t)c * 8 <= cw) {
+          qlh[packed.size()] = q;
+          qoh[packed.size()] = total;
+          packed.push_back(q);
+          total += c;
+          q++;
+          continue;
+        }
+        int qb = q + 1;  // a run of dense queries
+        while (qb < nq && !is_outside[qb] &&
+               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * 8 <= cw))
+          qb++;
+        RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4,
+                                   H.bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4, cw * 4,
+                                   (size_t)(qb - q), cudaMemcpyDeviceToHost, H.copy));
+        H.last_d2h += cw * 4 * (uint64_t)(qb - q);
+        q = qb;
+      }
+      if (packed.empty()) return;
+      const int np = (int)packed.size();
+      const int ds = r % 2, hs = r % 3;
+      gate.wait_free(hs);
+      int32_t *qld = H.ql + (size_t)nq * r;
+      uint64_t *qod = H.qoff + (size_t)nq * r;
+      RTS_CUDA(cudaMemcpyAsync(qld, qlh, np * sizeof(int32_t), cudaMemcpyHostToDevice, H.compute));
+      RTS_CUDA(cudaMemcpyAsync(qod, qoh, np * sizeof(uint64_t), cudaMemcpyHostToDevice, H.compute));
+      H.last_h2d += (uint64_t)np * (sizeof(int32_t) + sizeof(uint64_t));
+      if (r >= 2) RTS_CUDA(cudaStreamWaitEvent(H.compute, ev(r - 2, 4), 0));  // the device slot's last copy
+      rts::pack_kernel<<<np, rts::kSparseThreads, 0, H.compute>>>(H.bitmaps, stride_words, w0, w1, qld, qod,
+                                                                H.pairs[ds]);
+      ctx->launches++;
+      RTS_CUDA(cudaEventRecord(ev(r, 3), H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, ev(r, 3), 0));
+      if (total)
+        RTS_CUDA(cudaMemcpyAsync(H.pairs_host[hs], H.pairs[ds], total * sizeof(uint2), cudaMemcpyDeviceToHost,
+                                 H.copy));
+      H.last_d2h += total * sizeof(uint2);
+      RTS_CUDA(cudaEventRecord(ev(r, 4), H.copy));
+      const int tasks = std::min(np, pool->size());
+      gate.add(hs, tasks);
+      cudaEvent_t e = ev(r, 4);
+      const uint2 *ph = H.pairs_host[hs];
+      const int dev = ctx->device;
+      for (int t = 0; t < tasks; t++)
+        pool->post([=, &gate] {
+          cudaSetDevice(dev);
+          cudaEventSynchronize(e);
+          for (int j = t; j < np; j += tasks) {
+            const uint64_t a = qoh[j], b = j + 1 < np ? qoh[j + 1] : total;
+            rts::expand_pairs(host_bitmaps + (uint64_t)qlh[j] * stride_words + w0, cw, ph + a, b - a);
+          }
+          gate.done(hs);
+        });
+    };
     for (int r = 0; r < nchunks; r++) {
       const uint64_t r0 = (uint64_t)r * chunk_rows, r1 = std::min<uint64_t>(nrows, r0 + chunk_rows);
       for (int c = 0; c < ncols; c++)
         RTS_CUDA(cudaMemcpyAsync(H.cols + cstride * c + r0, host_cols[c] + r0, (r1 - r0) * 4,
                                  cudaMemcpyHostToDevice, H.up));
-      RTS_CUDA(cudaEventRecord(H.ev[2 * r], H.up));
-      RTS_CUDA(cudaStreamWaitEvent(H.compute, H.ev[2 * r], 0));
+      RTS_CUDA(cudaEventRecord(ev(r, 0), H.up));
+      RTS_CUDA(cudaStreamWaitEvent(H.compute, ev(r, 0), 0));
       if (!inside.empty())
         ctx->launches += rts::launch_plan(ctx, plan, dev_blob, H.bitmaps, stride_words, H.counts, r0, r1, pre,
                                           pre_bytes, H.compute);
-      RTS_CUDA(cudaEventRecord(H.ev[2 * r + 1], H.compute));
-      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * r + 1], 0));
+      RTS_CUDA(cudaEventRecord(ev(r, 1), H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, ev(r, 1), 0));
       const uint64_t w0 = r0 / 32, w1 = r1 == nrows ? words : r1 / 32;
-      if (nq > 0)
-        RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + w0, stride_words * 4, H.bitmaps + w0, stride_words * 4,
-                                   (w1 - w0) * 4, (size_t)nq, cudaMemcpyDeviceToHost, H.copy));
+      if (sparse && w1 - w0 >= rts::kSparseMinWords) {
+        rts::nnz_kernel<<<nq, rts::kSparseThreads, 0, H.compute>>>(H.bitmaps, stride_words, w0, w1,
+                                                                   H.nnz + (size_t)nq * r);
+        ctx->launches++;
+        RTS_CUDA(cudaMemcpyAsync(H.nnz_host + (size_t)nq * r, H.nnz + (size_t)nq * r, (size_t)nq * 4,
+                                 cudaMemcpyDeviceToHost, H.compute));
+        H.last_d2h += (uint64_t)nq * 4;
+        RTS_CUDA(cudaEventRecord(ev(r, 2), H.compute));
+      }
+      if (r >= 1) finish(r - 1);  // while chunk r runs
     }
+    if (nq > 0) finish(nchunks - 1);
     // Queries outside the batch kernels read the whole table: after the last
     // upload (ordered on the compute stream), then their whole bitmaps.
     if (!outside.empty()) {
       ctx->launches += rts::launch_outside(ctx, norm, outside, nullptr, H.bitmaps, stride_words, H.counts, H.compute);
-      RTS_CUDA(cudaEventRecord(H.ev[2 * nchunks], H.compute));
-      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * nchunks], 0));
-      for (int q : outside)
+      RTS_CUDA(cudaEventRecord(H.ev[kEv * nchunks], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[kEv * nchunks], 0));
+      for (int q : outside) {
         RTS_CUDA(cudaMemcpyAsync(host_bitmaps + (uint64_t)q * stride_words, H.bitmaps + (uint64_t)q * stride_words,
                                  words * 4, cudaMemcpyDeviceToHost, H.copy));
+        H.last_d2h += words * 4;
+      }
     }
     if (blob_done) RTS_CUDA(cudaEventRecord(blob_done, H.compute));
     if (pre) rts::context_pre_done(ctx, H.compute);
     RTS_CUDA(cudaGetLastError());
     if (nq > 0) {
-      RTS_CUDA(cudaEventRecord(H.ev[2 * nchunks], H.compute));
-      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[2 * nchunks], 0));
+      RTS_CUDA(cudaEventRecord(H.ev[kEv * nchunks], H.compute));
+      RTS_CUDA(cudaStreamWaitEvent(H.copy, H.ev[kEv * nchunks], 0));
       RTS_CUDA(cudaMemcpyAsync(host_counts, H.counts, (size_t)nq * 8, cudaMemcpyDeviceToHost, H.copy));
     }
     RTS_CUDA(cudaStreamSynchronize(H.copy));
     RTS_CUDA(cudaStreamSynchronize(H.compute));
     RTS_CUDA(cudaStreamSynchronize(H.up));
+    pool.reset();  // every packed query expanded
     return RTS_OK;
   } catch (const rts::Error &e) {
     ctx->err = e.what();
@@ -1637,6 +1811,14 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     ctx->err = e.what();
     return rts::set_thread_error(RTS_ERR_NOMEM, e.what());
   }
+}
+
+extern "C" rts_status rts_host_transfer_bytes(const rts_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes) {
+  if (!ctx || !h2d_bytes || !d2h_bytes) return rts::set_thread_error(RTS_ERR_ARG, "null argument");
+  const rts::HostBatchBuffers *H = ctx->host_batch;
+  *h2d_bytes = H ? H->last_h2d : 0;
+  *d2h_bytes = H ? H->last_d2h : 0;
+  return RTS_OK;
 }
 
 extern "C" rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, const int32_t *offsets, int32_t nq,

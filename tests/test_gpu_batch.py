@@ -316,6 +316,41 @@ def test_batch_host_buffers_many_chunks_and_a_refused_query(ctx):
     assert ctx.nrows == 1000
 
 
+def test_batch_host_sparse_chunks_are_expanded(ctx):
+    """Row chunks whose bitmap words are mostly zero leave the device as
+    (word, value) pairs that host threads expand: into buffers filled with
+    ones beforehand, every bitmap (very selective, dense and outside-kernel
+    queries mixed, four chunks) equals the device path's, the padding after
+    each bitmap is untouched, and fewer bytes crossed than whole bitmaps."""
+    n = (1 << 24) + 12_345
+    cols = [D.uniform(n, 700), D.zipf(n, 701, 1.3), D.uniform(n, 702, 1 << 20)]
+    s0 = np.sort(cols[0])
+    qs = D.batch_queries(cols, 200, seed=19)
+    rng = np.random.default_rng(20)
+    for k in (3, 40, 500, 4000, 30_000):  # 3 .. 30000 matching rows of column 0
+        i = int(rng.integers(0, n - k))
+        qs.append([(0, int(s0[i]), int(s0[i + k - 1]))])
+        qs.append([(0, int(s0[i]), int(s0[i + k - 1])), (2, 0, 1 << 19)])
+    qs.append([(1, 0, 0xFFFFFFFF)])  # every row
+    qs.append([(0, 5, 4)])           # empty
+    words = R.bitmap_words(n)
+    stride = words + 7
+    host = np.full((len(qs), stride), 0xFFFFFFFF, dtype=np.uint32)
+    bms, counts = ctx.scan_batch_host(cols, qs, host_bitmaps=host, stride_words=stride)
+    h2d, d2h = ctx.host_transfer_bytes()
+    ctx.load_columns(cols)
+    want = run_batch(ctx, qs, "batch")
+    for i in range(len(qs)):
+        assert int(counts[i]) == want[i][1], (i, qs[i])
+        assert np.array_equal(bms[i, :words], want[i][0]), (i, qs[i])
+        assert (bms[i, words:] == 0xFFFFFFFF).all(), i
+    for i in range(len(qs) - 12, len(qs)):
+        ref, rcnt = expect(cols, qs[i])
+        assert want[i][1] == rcnt and np.array_equal(want[i][0], ref), i
+    assert h2d >= 4 * n * len(cols)
+    assert d2h < len(qs) * words * 4, (d2h, len(qs) * words * 4)
+
+
 @pytest.mark.parametrize("nq", [1, 7, 100, 200, 400])
 def test_prepared_batch_graph_replays_match(ctx, nq):
     """Graph replays of each pass shape: a fused scan (1 query), term by term
