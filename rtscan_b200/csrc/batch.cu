@@ -142,7 +142,7 @@ __device__ __forceinline__ uint32_t position(const BatchPass &p, const uint32_t 
 // passes' table word offsets for it from one entry of a per-column map.
 // The passes then read four 16-bit offsets per row instead of searching
 // (batch4_kernel with PRE).  Pass column c is union column c.
-constexpr int kMaxPrePasses = 4;
+constexpr int kMaxPrePasses = kMaxSharedPasses;
 constexpr uint32_t kPreMaxBuckets = 4096;  // per union column
 
 // A union column: its m sorted distinct boundaries B, their bucket index and

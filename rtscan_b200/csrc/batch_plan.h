@@ -86,7 +86,9 @@ const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan);
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out,
                       uint64_t stride_words, unsigned long long *counts, uint64_t row_begin, uint64_t row_end,
                       void *scratch, size_t scratch_bytes, cudaStream_t s);
-// Scratch bytes that launch_batch_plan needs for `rows` rows (0: none).
+// Scratch bytes that launch_batch_plan needs for `rows` rows (0: none); at
+// most kMaxSharedPasses * (rows + 1) * 8 for any plan.
 size_t batch_plan_scratch_bytes(const BatchPlan &plan, uint64_t rows);
+constexpr int kMaxSharedPasses = 4;
 
 }  // namespace rts
