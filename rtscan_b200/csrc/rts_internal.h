@@ -122,6 +122,8 @@ void launch_bitmap_count(const uint32_t *bm, uint64_t nbits, unsigned long long 
 cudaError_t preload_separate_scan_kernels();
 void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count,
                        int sm_count, cudaStream_t s);
+// counts[slots[i]] = 0 for i < n, in one launch per 512 slots.
+void launch_zero_counts(unsigned long long *counts, const int32_t *slots, int n, cudaStream_t s);
 
 // ---- BinDex on the GPU (bindex.cu) ----
 struct GpuBinDex {

@@ -18,6 +18,9 @@
 // the warp then stores its 32 words as one 128-byte segment.  The kernel is
 // HBM-bound: 4 bytes per row per column read plus 1/8 byte per row written.
 #include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "rts_internal.h"
 
@@ -307,6 +310,28 @@ cudaError_t preload_separate_scan_kernels() {
   max_blocks<1, true>(1);  // the occupancy queries that size the fused-scan grids, cached here
   max_blocks<0, false>(1);
   return cudaSuccess;
+}
+
+namespace {
+constexpr int kZeroSlotsPerLaunch = 512;
+struct ZeroSlots {
+  unsigned long long *counts;
+  int n;
+  int32_t slot[kZeroSlotsPerLaunch];
+};
+__global__ void zero_slots_kernel(const __grid_constant__ ZeroSlots z) {
+  for (int i = threadIdx.x; i < z.n; i += blockDim.x) z.counts[z.slot[i]] = 0;
+}
+}  // namespace
+
+void launch_zero_counts(unsigned long long *counts, const int32_t *slots, int n, cudaStream_t s) {
+  for (int a = 0; a < n; a += kZeroSlotsPerLaunch) {
+    ZeroSlots z;
+    z.counts = counts;
+    z.n = std::min(kZeroSlotsPerLaunch, n - a);
+    memcpy(z.slot, slots + a, (size_t)z.n * sizeof(int32_t));
+    zero_slots_kernel<<<1, 256, 0, s>>>(z);
+  }
 }
 
 void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long long *count, int sm_count,

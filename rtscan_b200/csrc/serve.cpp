@@ -119,6 +119,18 @@ struct rts_server {
   std::atomic<bool> stop{false};
   std::thread worker;
 
+  // Events that slots wait on, with the number of slots waiting on each
+  // (the requests finishing at one step share one event).
+  std::unordered_map<cudaEvent_t, int> ev_refs;
+  void hold(cudaEvent_t e) { ev_refs[e]++; }
+  void drop(cudaEvent_t e) {
+    auto it = ev_refs.find(e);
+    if (it != ev_refs.end() && --it->second == 0) {
+      ev_refs.erase(it);
+      put_event(e);
+    }
+  }
+
   cudaEvent_t get_event() {
     if (!event_pool.empty()) {
       cudaEvent_t e = event_pool.back();
@@ -164,8 +176,10 @@ struct rts_server {
   }
   PlanBuf *current_pb = nullptr;
 
-  // Admit queued requests into free slots (mu held).
+  // Admit queued requests into free slots (mu held); their counts are
+  // zeroed by one launch.
   void admit() {
+    std::vector<int32_t> fresh;
     while (!queue.empty() && !free_slots.empty()) {
       Request r = std::move(queue.front());
       queue.pop_front();
@@ -185,21 +199,37 @@ struct rts_server {
         ctx->launches += rts::launch_outside(ctx, one, {sl}, nullptr, bitmaps, stride, counts, stream);
         finish(sl);
       } else {
-        RTS_CUDA(cudaMemsetAsync(counts + sl, 0, 8, stream));
+        fresh.push_back(sl);
         S.state = ACTIVE;
         active_version++;
       }
+    }
+    if (!fresh.empty()) {
+      rts::launch_zero_counts(counts, fresh.data(), (int)fresh.size(), stream);
+      ctx->launches += ((int)fresh.size() + 511) / 512;
     }
   }
 
   // Queue the copy of slot sl's count to the host and the event that marks
   // the slot done, behind every launch that writes it (mu held).
-  void finish(int sl) {
-    Slot &S = slots[sl];
-    RTS_CUDA(cudaMemcpyAsync(host_counts + sl, counts + sl, 8, cudaMemcpyDeviceToHost, stream));
-    S.ev = get_event();
-    RTS_CUDA(cudaEventRecord(S.ev, stream));
-    S.state = FINISHING;
+  void finish(int sl) { finish_all(&sl, 1); }
+
+  // The same for the slots finishing at one step: one copy of the counts
+  // from the lowest to the highest of them (the others' device counts are
+  // unchanged or not yet read) and one event they share (mu held).
+  void finish_all(const int *sl, int n) {
+    if (n == 0) return;
+    const int lo = *std::min_element(sl, sl + n), hi = *std::max_element(sl, sl + n);
+    RTS_CUDA(cudaMemcpyAsync(host_counts + lo, counts + lo, (size_t)(hi - lo + 1) * 8, cudaMemcpyDeviceToHost,
+                             stream));
+    cudaEvent_t e = get_event();
+    RTS_CUDA(cudaEventRecord(e, stream));
+    for (int i = 0; i < n; i++) {
+      Slot &S = slots[sl[i]];
+      S.ev = e;
+      hold(e);
+      S.state = FINISHING;
+    }
   }
 
   // Slots cancelled while active get their release event here, after every
@@ -208,6 +238,7 @@ struct rts_server {
     for (auto &S : slots)
       if (S.state == CANCELLING && !S.ev) {
         S.ev = get_event();
+        hold(S.ev);
         RTS_CUDA(cudaEventRecord(S.ev, stream));
       }
   }
@@ -246,29 +277,30 @@ struct rts_server {
     if (current_pb) RTS_CUDA(cudaEventRecord(current_pb->done, stream));
     steps++;
     cursor = (cursor + 1) % nseg;
-    bool changed = false;
+    std::vector<int> done_now;
     for (int sl : plan_slots) {
       Slot &S = slots[sl];
       if (S.state != ACTIVE) continue;  // cancelled since the plan was made
-      if (++S.segs_done == nseg) {
-        finish(sl);
-        changed = true;
-      }
+      if (++S.segs_done == nseg) done_now.push_back(sl);
     }
-    if (changed) active_version++;
+    finish_all(done_now.data(), (int)done_now.size());
+    if (!done_now.empty()) active_version++;
   }
 
   // Mark finished requests done (mu held).
   void reap() {
     bool any = false;
+    std::unordered_map<cudaEvent_t, cudaError_t> state;  // each shared event queried once
     for (size_t i = 0; i < slots.size(); i++) {
       Slot &S = slots[i];
       if (S.state != FINISHING && S.state != CANCELLING) continue;
       if (!S.ev) continue;  // a cancel not fenced yet
-      cudaError_t e = cudaEventQuery(S.ev);
+      auto st = state.find(S.ev);
+      if (st == state.end()) st = state.emplace(S.ev, cudaEventQuery(S.ev)).first;
+      const cudaError_t e = st->second;
       if (e == cudaErrorNotReady) continue;
       if (e != cudaSuccess) throw rts::Error(RTS_ERR_CUDA, std::string("server step: ") + cudaGetErrorString(e));
-      put_event(S.ev);
+      drop(S.ev);
       S.ev = nullptr;
       if (S.state == CANCELLING) {
         S.state = FREE;
@@ -359,8 +391,7 @@ struct rts_server {
     }
     for (auto e : inflight) cudaEventDestroy(e);
     for (auto e : event_pool) cudaEventDestroy(e);
-    for (auto &S : slots)
-      if (S.ev) cudaEventDestroy(S.ev);
+    for (auto &kv : ev_refs) cudaEventDestroy(kv.first);  // each slot event once
     if (bitmaps) cudaFree(bitmaps);
     if (counts) cudaFree(counts);
     if (host_counts) cudaFreeHost(host_counts);
