@@ -1661,7 +1661,9 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     // query; a packed query has at most cw / 8 nonzero words in the chunk.
     const uint64_t cw_max = chunk_rows / 32;
     const bool sparse = nq > 0 && !inside.empty() && cw_max >= rts::kSparseMinWords;
-    const uint64_t max_pairs = sparse ? (uint64_t)nq * (cw_max / 8) : 0;
+    // pairs per chunk: every packed query's, up to kSparseMaxPairs (a query
+    // that would pass it is sent whole)
+    const uint64_t max_pairs = sparse ? std::min<uint64_t>((uint64_t)nq * (cw_max / 8), rts::kSparseMaxPairs) : 0;
     if (sparse) {
       rts::ensure(H.nnz, H.nnz_cap, (size_t)nq * nchunks);
       rts::ensure_host(H.nnz_host, H.nnz_host_cap, (size_t)nq * nchunks);
@@ -1700,7 +1702,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
           continue;
         }
         const uint32_t c = try_pack ? H.nnz_host[(size_t)nq * r + q] : 0u;
-        if (try_pack && (uint64_t)c * 8 <= cw) {
+        if (try_pack && (uint64_t)c * 8 <= cw && total + c <= max_pairs) {
           qlh[packed.size()] = q;
           qoh[packed.size()] = total;
           packed.push_back(q);
@@ -1710,7 +1712,8 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
         }
         int qb = q + 1;  // a run of dense queries
         while (qb < nq && !is_outside[qb] &&
-               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * 8 <= cw))
+               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * 8 <= cw &&
+                 total + H.nnz_host[(size_t)nq * r + qb] <= max_pairs))
           qb++;
         RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4,
                                    H.bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4, cw * 4,

@@ -25,6 +25,7 @@
 constexpr int kSparseThreads = 256;
 constexpr int kSparseWordsPerThread = 4;
 constexpr uint64_t kSparseMinWords = 4096;  // chunks of fewer words per query are sent whole
+constexpr uint64_t kSparseMaxPairs = 1ull << 24;  // pairs of one chunk (128 MiB per staging slot)
 
 // Nonzero words of query q's bitmap in [w0, w1): one block per query.
 __global__ void __launch_bounds__(kSparseThreads) nnz_kernel(const uint32_t *bm, uint64_t stride, uint64_t w0,
