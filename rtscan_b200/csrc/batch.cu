@@ -204,7 +204,7 @@ __host__ __device__ __forceinline__ uint32_t pre_position(const PreCol &pc, cons
   return pos;
 }
 
-constexpr int kPreThreads = 512;
+constexpr int kPreThreads = 1024;  // two-pass batches: two blocks per SM, 64 warps over two table copies
 constexpr int kPrePairs = 2;  // row pairs per thread and iteration: their loads and searches overlap
 constexpr uint64_t kPreTile = (uint64_t)kPreThreads * kPrePairs * 2;  // rows of one block iteration
 
@@ -217,7 +217,7 @@ __host__ __device__ __forceinline__ uint64_t pre_stride(uint64_t rows) { return 
 // 8-byte aligned columns (P.vec) load each column's pair as one uint2 and
 // store each pass's pair as one uint4, without per-row checks.
 template <int U, int NW>
-__global__ void __launch_bounds__(kPreThreads) pre_kernel(const __grid_constant__ PreParams P) {
+__global__ void __launch_bounds__(kPreThreads, NW == 1 ? 2 : 1) pre_kernel(const __grid_constant__ PreParams P) {
   extern __shared__ __align__(16) uint32_t smem[];
   for (uint32_t i = threadIdx.x; i < P.blob_words; i += blockDim.x) smem[i] = __ldg(P.blob + i);
   __syncthreads();

@@ -316,6 +316,24 @@ def test_batch_host_buffers_many_chunks_and_a_refused_query(ctx):
     assert ctx.nrows == 1000
 
 
+def test_four_passes_share_positions(ctx):
+    """1600 queries over four columns make four 512-slot passes (the table
+    budget holds about 400 queries each) that share one position search per
+    row, two map words per union position; every bitmap and count equals
+    one query per launch, and a sample the scalar filter."""
+    n = (1 << 21) + 77
+    cols = [D.zipf(n, 240, 1.1), D.uniform(n, 241), D.normal(n, 242), D.zipf(n, 243, 1.5)]
+    ctx.load_columns(cols)
+    qs = D.batch_queries(cols, 1600, seed=33, min_cols=2, max_cols=4)
+    want = run_batch(ctx, qs, "each")
+    got = run_batch(ctx, qs, "batch")
+    for i in range(len(qs)):
+        assert got[i][1] == want[i][1] and np.array_equal(got[i][0], want[i][0]), i
+    for i in (0, 700, 1599):
+        ref, rcnt = expect(cols, qs[i])
+        assert want[i][1] == rcnt and np.array_equal(want[i][0], ref), i
+
+
 def test_batch_host_sparse_chunks_are_expanded(ctx):
     """Row chunks whose bitmap words are mostly zero leave the device as
     (word, value) pairs that host threads expand: into buffers filled with
