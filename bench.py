@@ -580,6 +580,7 @@ def run(args):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": round(ms_step, 5),
+        "step_ms": {"min": round(min(per), 4), "median": round(statistics.median(per), 4), "max": round(max(per), 4)},
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
