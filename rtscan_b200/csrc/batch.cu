@@ -891,17 +891,23 @@ std::vector<uint32_t> pre_buckets(const std::vector<uint32_t> &B, PreCol &pc) {
     t.L = L;
     t.nbk = nbk;
     double cost = 0;
-    for (uint32_t lo = 0; lo < m;) {
-      const uint32_t k = pre_bucket(t, B[lo]);
-      uint32_t hi = lo + 1;
-      while (hi < m && pre_bucket(t, B[hi]) == k) hi++;
+    auto close = [&](uint32_t k, uint32_t lo, uint32_t hi) {  // boundaries [lo, hi) in bucket k
       const uint64_t start = (uint64_t)pc.origin + pre_bucket_start(M, L, k);
       const uint32_t n = hi - lo - (B[lo] == start ? 1u : 0u);
       uint32_t steps = 0;
       for (uint32_t r = n; r; r >>= 1) steps++;
       cost += (double)steps * (hi - lo);
-      lo = hi;
+    };
+    uint32_t lo = 0, k = pre_bucket(t, B[0]);
+    for (uint32_t i = 1; i < m; i++) {
+      const uint32_t ki = pre_bucket(t, B[i]);
+      if (ki != k) {
+        close(k, lo, i);
+        lo = i;
+        k = ki;
+      }
     }
+    close(k, lo, m);
     return cost;
   };
   const uint32_t vmax = B.back() - pc.origin;
@@ -997,9 +1003,15 @@ void plan_shared_positions(BatchPlan &plan) {
       const int s = (int)(std::find(src.col, src.col + U, plan.passes[which[0]].bp.col[c]) - src.col);
       move_column(ordered[q], c, src, s);
     }
+    // each pass's boundaries are sorted: merge them into the union
     const uint32_t *blob = plan.blob.data() + plan.passes[which[q]].off;
-    for (int c = 0; c < U; c++)
-      Bu[c].insert(Bu[c].end(), blob + ordered[q].bnd_off[c], blob + ordered[q].bnd_off[c] + ordered[q].m[c]);
+    for (int c = 0; c < U; c++) {
+      const uint32_t *Bp = blob + ordered[q].bnd_off[c];
+      std::vector<uint32_t> merged(Bu[c].size() + ordered[q].m[c]);
+      merged.resize(std::set_union(Bu[c].begin(), Bu[c].end(), Bp, Bp + ordered[q].m[c], merged.begin()) -
+                    merged.begin());
+      Bu[c].swap(merged);
+    }
   }
   PreParams P;
   memset(&P, 0, sizeof P);
@@ -1007,9 +1019,7 @@ void plan_shared_positions(BatchPlan &plan) {
   P.npass = npass;
   std::vector<uint32_t> ub;  // offsets relative to its own start
   for (int c = 0; c < U; c++) {
-    std::vector<uint32_t> &B = Bu[c];
-    std::sort(B.begin(), B.end());
-    B.erase(std::unique(B.begin(), B.end()), B.end());
+    const std::vector<uint32_t> &B = Bu[c];  // sorted and distinct
     if (B.size() > 0xFFFFu) return;  // bucket entries hold 16-bit positions
     PreCol &pc = P.c[c];
     pc.col = ordered[0].col[c];
