@@ -189,7 +189,8 @@ def test_batch_alone_and_in_the_mix(ctx):
         assert np.array_equal(alone[0], mixed[i][0])
 
 
-@pytest.mark.parametrize("cfg", [(4, 16, 512, 136 * 1024), (4, 16, 100, 136 * 1024), (4, 16, 512, 8 * 1024),
+@pytest.mark.parametrize("cfg", [(4, 16, 512, 136 * 1024), (4, 16, 256, 136 * 1024), (4, 16, 100, 136 * 1024),
+                                 (4, 16, 512, 8 * 1024),
                                  (4, 8, 512, 136 * 1024), (4, 8, 512, 56 * 1024), (4, 8, 256, 56 * 1024),
                                  (4, 8, 128, 56 * 1024), (4, 8, 100, 136 * 1024),
                                  (3, 16, 256, 88 * 1024), (3, 16, 64, 16 * 1024), (3, 8, 256, 40 * 1024),
