@@ -1027,15 +1027,23 @@ def served_leg(torch, R, D, ctx, dev, rank, args):
             nq = max(1, int(rate * seconds))
             qs = R.prepare(D.batch_queries(samples, nq, seed=rate))
             arr = np.cumsum(np.random.default_rng(rate).exponential(1.0 / rate, size=nq))
+            st0 = srv.stats()
             t0 = time.perf_counter()
             lat = srv.replay(qs, arr)
             wall = time.perf_counter() - t0
+            st1 = srv.stats()
             ok = lat[lat >= 0]
+            steps, plans = st1["steps"] - st0["steps"], st1["plans"] - st0["plans"]
             out["rates"].append({"offered_qps": rate, "queries": nq, "achieved_qps": round(len(ok) / wall, 1),
                                  "rejected": int((lat < 0).sum()),
                                  "p50_ms": round(float(np.percentile(ok, 50)), 3),
                                  "p99_ms": round(float(np.percentile(ok, 99)), 3),
-                                 "p999_ms": round(float(np.percentile(ok, 99.9)), 3)})
+                                 "p999_ms": round(float(np.percentile(ok, 99.9)), 3),
+                                 # the worker's steps (one segment each) and plans in the replay, and the
+                                 # host time of a plan: planning slower than a step bounds the server
+                                 "steps": steps, "plans": plans,
+                                 "plan_ms_mean": round((st1["plan_ms_total"] - st0["plan_ms_total"]) / max(plans, 1), 3),
+                                 "ms_per_step": round(wall * 1e3 / max(steps, 1), 3)})
         # the highest offered rate the server kept up with: every request
         # admitted (none rejected) and completions within 2 % of the offer
         kept = [r for r in out["rates"] if r["rejected"] == 0 and r["achieved_qps"] >= 0.98 * r["offered_qps"]]

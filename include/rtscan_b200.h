@@ -311,13 +311,15 @@ typedef struct rts_server_config {
   int32_t max_active;         /* result slots (bitmap + count each); default 512 */
   int32_t max_queue;          /* requests waiting for a slot before RTS_ERR_FULL; default 65536 */
   uint64_t segment_rows;      /* rows per scan step, a multiple of 4096; default 2^22 */
-  int32_t max_inflight_steps; /* steps queued on the GPU at once; default 2 */
+  int32_t max_inflight_steps; /* steps queued on the GPU at once; default 3 */
 } rts_server_config;
 
 typedef struct rts_server_stats {
   uint64_t submitted, completed, rejected, cancelled, steps, queued;
   uint32_t active;
   double p50_ms, p99_ms, p999_ms, max_ms, mean_ms; /* submit-to-done latency of completed requests */
+  uint64_t plans;       /* batch plans made for the active set */
+  double plan_ms_total; /* host time spent making and uploading them */
 } rts_server_stats;
 
 /* cfg may be NULL (defaults); zero fields take their defaults. */

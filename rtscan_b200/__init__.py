@@ -62,7 +62,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("cancelled", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("queued", ctypes.c_uint64),
                 ("active", ctypes.c_uint32), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
-                ("p999_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double)]
+                ("p999_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("plans", ctypes.c_uint64), ("plan_ms_total", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -756,6 +757,10 @@ struct BatchPlan {
   // shared positions of the passes with a pre_slot (npass 0: none)
   PreParams pre;
   size_t pre_off = 0;  // word offset of the union boundaries, buckets and maps in `blob`
+  // batch_plan_drop: per query index, where its slot is (built at the first
+  // drop): the blob word of a table-pass slot, or -(1 + pass) for a
+  // term-by-term pass, or INT64_MIN when the plan does not hold it
+  std::vector<int64_t> where;
 };
 
 // Answer the queries that do not run in the batch kernel (empty, no
@@ -1486,6 +1491,44 @@ BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, c
 }
 
 const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan) { return plan.blob; }
+
+void batch_plan_drop(BatchPlan &plan, int qi, std::vector<uint32_t> &blob_words) {
+  if (plan.where.empty()) {
+    int maxq = 0;
+    for (const auto &b : plan.passes) {
+      if (b.few) {
+        for (int j = 0; j < b.fp.nq; j++) maxq = std::max(maxq, b.fp.slot_query[j]);
+      } else {
+        const int32_t *slot = reinterpret_cast<const int32_t *>(plan.blob.data() + b.off + b.bp.slot_off);
+        for (int sl = 0; sl < 32 * b.groups; sl++) maxq = std::max(maxq, slot[sl]);
+      }
+    }
+    plan.where.assign((size_t)maxq + 1, INT64_MIN);
+    for (size_t i = 0; i < plan.passes.size(); i++) {
+      const auto &b = plan.passes[i];
+      if (b.few) {
+        for (int j = 0; j < b.fp.nq; j++)
+          if (b.fp.slot_query[j] >= 0) plan.where[b.fp.slot_query[j]] = -1 - (int64_t)i;
+      } else {
+        const size_t base = b.off + b.bp.slot_off;
+        const int32_t *slot = reinterpret_cast<const int32_t *>(plan.blob.data() + base);
+        for (int sl = 0; sl < 32 * b.groups; sl++)
+          if (slot[sl] >= 0) plan.where[slot[sl]] = (int64_t)(base + sl);
+      }
+    }
+  }
+  if (qi < 0 || (size_t)qi >= plan.where.size() || plan.where[qi] == INT64_MIN) return;
+  const int64_t w = plan.where[qi];
+  plan.where[qi] = INT64_MIN;
+  if (w >= 0) {
+    plan.blob[w] = 0xFFFFFFFFu;
+    blob_words.push_back((uint32_t)w);
+    return;
+  }
+  FewPass &f = plan.passes[(size_t)(-1 - w)].fp;
+  for (int j = 0; j < f.nq; j++)
+    if (f.slot_query[j] == qi) f.slot_query[j] = -1;
+}
 
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out, uint64_t stride_words,
                       unsigned long long *counts, uint64_t row_begin, uint64_t row_end, void *scratch,

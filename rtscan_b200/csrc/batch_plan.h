@@ -86,6 +86,13 @@ const std::vector<uint32_t> &batch_plan_blob(const BatchPlan &plan);
 int launch_batch_plan(rts_ctx *ctx, BatchPlan &plan, const uint32_t *dev_blob, uint32_t *out,
                       uint64_t stride_words, unsigned long long *counts, uint64_t row_begin, uint64_t row_end,
                       void *scratch, size_t scratch_bytes, cudaStream_t s);
+// Stop the plan from writing query qi's bitmap and count (a request that
+// finished or was cancelled while the plan keeps running): term-by-term and
+// fused passes are changed in the plan; for table passes the plan blob's
+// slot entry becomes -1 and its word offset is appended to `blob_words`,
+// the words the caller must also set to 0xFFFFFFFF in the uploaded blob
+// before the next launch.  A query the plan does not hold is ignored.
+void batch_plan_drop(BatchPlan &plan, int qi, std::vector<uint32_t> &blob_words);
 // Scratch bytes that launch_batch_plan needs for `rows` rows (0: none); at
 // most kMaxSharedPasses * (rows + 1) * 8 for any plan.
 size_t batch_plan_scratch_bytes(const BatchPlan &plan, uint64_t rows);

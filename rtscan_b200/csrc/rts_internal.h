@@ -124,6 +124,8 @@ void launch_fill_range(uint32_t *out, uint64_t nrows, bool ones, unsigned long l
                        int sm_count, cudaStream_t s);
 // counts[slots[i]] = 0 for i < n, in one launch per 512 slots.
 void launch_zero_counts(unsigned long long *counts, const int32_t *slots, int n, cudaStream_t s);
+// base[offs[i]] = value for i < n, in one launch per 512 words.
+void launch_set_words(uint32_t *base, const uint32_t *offs, int n, uint32_t value, cudaStream_t s);
 
 // ---- BinDex on the GPU (bindex.cu) ----
 struct GpuBinDex {

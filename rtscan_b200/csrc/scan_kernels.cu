@@ -324,6 +324,29 @@ __global__ void zero_slots_kernel(const __grid_constant__ ZeroSlots z) {
 }
 }  // namespace
 
+namespace {
+struct SetWords {
+  uint32_t *base;
+  uint32_t value;
+  int n;
+  uint32_t off[kZeroSlotsPerLaunch];
+};
+__global__ void set_words_kernel(const __grid_constant__ SetWords z) {
+  for (int i = threadIdx.x; i < z.n; i += blockDim.x) z.base[z.off[i]] = z.value;
+}
+}  // namespace
+
+void launch_set_words(uint32_t *base, const uint32_t *offs, int n, uint32_t value, cudaStream_t s) {
+  for (int a = 0; a < n; a += kZeroSlotsPerLaunch) {
+    SetWords z;
+    z.base = base;
+    z.value = value;
+    z.n = std::min(kZeroSlotsPerLaunch, n - a);
+    memcpy(z.off, offs + a, (size_t)z.n * sizeof(uint32_t));
+    set_words_kernel<<<1, 256, 0, s>>>(z);
+  }
+}
+
 void launch_zero_counts(unsigned long long *counts, const int32_t *slots, int n, cudaStream_t s) {
   for (int a = 0; a < n; a += kZeroSlotsPerLaunch) {
     ZeroSlots z;

@@ -12,20 +12,25 @@
 //     runs the batched kernel over one segment for every active request and
 //     then moves a cursor to the next segment, wrapping around.  A request
 //     admitted while the cursor is at segment c0 has seen every segment once
-//     when the cursor returns to c0; its count, accumulated per segment, and
-//     its bitmap are then final.  New arrivals join at the next step, so
-//     their work overlaps on the device with requests already running.
-//   * The worker thread plans the active set (mask tables) only when it
-//     changes, keeps at most `max_inflight_steps` steps queued on its stream,
-//     and marks a request done when the event recorded after its last step
-//     has completed.  Planning and the plan upload (which waits for the
-//     steps still reading the other plan buffer) run without the server
-//     lock, so submitters and pollers never wait behind them; the lock
-//     covers admission, the step's launches and the bookkeeping only.
-//   * A finished request's count is copied to pinned host memory on the
-//     scan stream right after its last step (one 8-byte copy each), so
-//     poll/wait/fetch read it without touching the device; a bitmap fetch
-//     copies outside the lock.
+//     when it has been in the scan for one segment of each; its count,
+//     accumulated per segment, and its bitmap are then final.  New arrivals
+//     join at the next plan, so their work overlaps on the device with
+//     requests already running.
+//   * The worker thread plans the active set (mask tables) when requests
+//     arrive, at most every kReplanSteps steps while the running plan still
+//     has requests, keeps at most `max_inflight_steps` steps queued on its
+//     stream, and marks a request done when the event recorded after its
+//     last step has completed.  A request that finishes or is cancelled
+//     leaves the running plan without a re-plan: its slot entries in the
+//     plan become -1 (one small launch per step), which every batch kernel
+//     skips.  Planning and the plan upload (which waits for the steps still
+//     reading the other plan buffer) run without the server lock, so
+//     submitters and pollers never wait behind them; the lock covers
+//     admission, the step's launches and the bookkeeping only.
+//   * The requests finishing at a step share one copy of their counts to
+//     pinned host memory and one event, queued right after the step, so
+//     poll/wait/fetch read a count without touching the device; a bitmap
+//     fetch copies outside the lock.
 // Requests the batched kernel does not take (an empty term, no constrained
 // column, more than eight columns) are answered in one launch at admission.
 #include <cuda_runtime.h>
@@ -102,6 +107,11 @@ struct rts_server {
   uint64_t next_ticket = 1;
   int cursor = 0;
   uint64_t active_version = 1, plan_version = 0;
+  uint64_t plan_step = 0;                // steps launched when the running plan was made
+  double last_plan_s = 0;                // host time of the last plan and upload
+  double step_s = 0;                     // moving average of the GPU's time per step
+  double last_retire = 0;
+  static constexpr uint64_t kReplanSteps = 2;
   rts::BatchPlanPtr plan;
   const uint32_t *plan_dev = nullptr;
   std::vector<int> plan_slots;
@@ -109,7 +119,8 @@ struct rts_server {
   std::vector<cudaEvent_t> event_pool;
 
   // statistics
-  uint64_t submitted = 0, completed = 0, rejected = 0, cancelled = 0, steps = 0;
+  uint64_t submitted = 0, completed = 0, rejected = 0, cancelled = 0, steps = 0, plans = 0;
+  double plan_s = 0;  // host time of the plans and their uploads
   std::vector<double> latencies;
   std::string fatal;
   // completions (ticket, done time) for a running replay
@@ -235,12 +246,33 @@ struct rts_server {
   // Slots cancelled while active get their release event here, after every
   // launch queued so far, some of which may still write them (mu held).
   void fence_cancels() {
-    for (auto &S : slots)
-      if (S.state == CANCELLING && !S.ev) {
-        S.ev = get_event();
-        hold(S.ev);
-        RTS_CUDA(cudaEventRecord(S.ev, stream));
-      }
+    std::vector<int> gone;
+    for (size_t i = 0; i < slots.size(); i++)
+      if (slots[i].state == CANCELLING && !slots[i].ev) gone.push_back((int)i);
+    if (gone.empty()) return;
+    unplan(gone);  // no later step writes them
+    for (int sl : gone) {
+      Slot &S = slots[sl];
+      S.ev = get_event();
+      hold(S.ev);
+      RTS_CUDA(cudaEventRecord(S.ev, stream));
+    }
+  }
+
+  // Take slots out of the running plan (mu held): their entries in the
+  // plan's slot maps become -1 (on the device by one launch, queued before
+  // the next step), and the steps stop counting segments for them.
+  void unplan(const std::vector<int> &gone) {
+    if (!plan || gone.empty()) return;
+    std::vector<uint32_t> words;
+    for (int sl : gone) rts::batch_plan_drop(*plan, sl, words);
+    if (!words.empty()) {
+      rts::launch_set_words(const_cast<uint32_t *>(plan_dev), words.data(), (int)words.size(), 0xFFFFFFFFu, stream);
+      ctx->launches += ((int)words.size() + 511) / 512;
+    }
+    plan_slots.erase(std::remove_if(plan_slots.begin(), plan_slots.end(),
+                                    [&](int sl) { return std::find(gone.begin(), gone.end(), sl) != gone.end(); }),
+                     plan_slots.end());
   }
 
   // The active set, and a copy of its queries when it differs from the
@@ -254,6 +286,14 @@ struct rts_server {
       if (slots[i].state == ACTIVE) active.push_back((int)i);
     if (active.empty()) return -1;
     if (plan_version == active_version) return 0;
+    // New arrivals join at the next plan.  When planning takes the host
+    // longer than the GPU takes for a step (a slow host, a large active
+    // set), plans are made at most every kReplanSteps steps while the
+    // running plan still has requests: between plans the worker launches
+    // steps back to back, so the GPU runs the steps queued during a plan's
+    // host work.  Otherwise every change is planned at once (a deferred plan
+    // carries its finished requests' slots one step longer).
+    if (plan && !plan_slots.empty() && steps - plan_step < kReplanSteps && last_plan_s > step_s) return 0;
     norm.assign(slots.size(), rts::NormQuery());
     for (int sl : active) norm[sl] = slots[sl].q;
     version = active_version;
@@ -284,7 +324,10 @@ struct rts_server {
       if (++S.segs_done == nseg) done_now.push_back(sl);
     }
     finish_all(done_now.data(), (int)done_now.size());
-    if (!done_now.empty()) active_version++;
+    // the plan keeps running without them; when planning is cheaper than a
+    // step, the next step gets a plan without their slots as well
+    unplan(done_now);
+    if (!done_now.empty() && last_plan_s <= step_s) active_version++;
   }
 
   // Mark finished requests done (mu held).
@@ -326,9 +369,17 @@ struct rts_server {
         // bound the steps queued on the stream, without holding the lock
         std::vector<cudaEvent_t> retired;
         while ((int)inflight.size() >= cfg.max_inflight_steps) {
+          // a step still running when the worker comes for it: the GPU, not
+          // the host, sets the pace, and the interval between two such
+          // finished steps is the GPU's time per step
+          const bool gpu_paced = cudaEventQuery(inflight.front()) == cudaErrorNotReady;
           RTS_CUDA(cudaEventSynchronize(inflight.front()));
           retired.push_back(inflight.front());
           inflight.pop_front();
+          const double t = now_s();
+          if (gpu_paced && last_retire > 0)
+            step_s = step_s > 0 ? 0.9 * step_s + 0.1 * (t - last_retire) : t - last_retire;
+          last_retire = gpu_paced ? t : 0;
         }
         uint64_t version = 0;
         int todo = -1;
@@ -342,6 +393,7 @@ struct rts_server {
           for (auto &S : slots)
             if (S.state == ACTIVE || S.state == FINISHING || S.state == CANCELLING) busy = true;
           if (!busy && queue.empty()) {
+            last_retire = 0;  // idle time is no step time
             cv_work.wait_for(lk, std::chrono::milliseconds(2));
             continue;
           }
@@ -353,11 +405,23 @@ struct rts_server {
           }
         }
         if (todo == 1) {  // plan and upload without the lock
+          const double t0 = now_s();
           rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget, false);
           upload(rts::batch_plan_blob(*p));
+          const double t1 = now_s();
+          std::lock_guard<std::mutex> lk(mu);
+          plans++;
+          plan_s += t1 - t0;
+          last_plan_s = t1 - t0;
           plan = std::move(p);
           plan_slots = active;
           plan_version = version;
+          plan_step = steps;
+          // requests cancelled while it was planned run no step of it
+          std::vector<int> gone;
+          for (int sl : active)
+            if (slots[sl].state != ACTIVE) gone.push_back(sl);
+          unplan(gone);
         }
         {
           std::lock_guard<std::mutex> lk(mu);
@@ -447,7 +511,7 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
     c.max_active = 512;
     c.max_queue = 1 << 16;
     c.segment_rows = 1ull << 22;
-    c.max_inflight_steps = 2;
+    c.max_inflight_steps = 3;
     if (cfg) {
       if (cfg->max_active > 0) c.max_active = cfg->max_active;
       if (cfg->max_queue > 0) c.max_queue = cfg->max_queue;
@@ -654,6 +718,8 @@ rts_status rts_server_get_stats(rts_server *srv, rts_server_stats *st) {
     }
     st->max_ms = mx * 1e3;
     st->mean_ms = srv->latencies.empty() ? 0 : sum / (double)srv->latencies.size() * 1e3;
+    st->plans = srv->plans;
+    st->plan_ms_total = srv->plan_s * 1e3;
     return RTS_OK;
   });
 }

@@ -155,3 +155,40 @@ def test_replay_stopped_by_a_refused_request_releases_its_slots(ctx, table):
             assert srv.fetch(tk, want_bitmap=False)[1] == alone(ctx, q)[1]
         lat = srv.replay(good, np.linspace(0, 0.01, len(good)))
         assert (lat > 0).all()
+
+
+def test_cancels_while_running_and_slots_reused(ctx, table):
+    """Requests cancelled while the scan runs them leave the running plan
+    without a re-plan; their slots are reused by later requests, whose
+    results (and every request not cancelled) equal the direct scan."""
+    ctx.load_columns(table)
+    qs = D.batch_queries(table, 240, seed=13)
+    want = [alone(ctx, q) for q in qs]
+    rng = np.random.default_rng(3)
+    with R.Server(ctx, max_active=24, segment_rows=1 << 17) as srv:
+        live = {}
+        cancelled = 0
+        for i, q in enumerate(qs):
+            live[srv.submit(q)] = i
+            if i % 3 == 2:  # cancel one of the requests submitted so far, running or queued
+                tk = list(live)[int(rng.integers(0, len(live)))]
+                try:
+                    srv.cancel(tk)
+                    live.pop(tk)
+                    cancelled += 1
+                except R.RtsError:
+                    pass  # already being fetched below, or done and released
+            # fetch whatever is done, so that slots free up for new requests
+            for tk in list(live):
+                done, _ = srv.poll(tk)
+                if done:
+                    bm, cnt = srv.fetch(tk)
+                    j = live.pop(tk)
+                    assert cnt == want[j][1] and np.array_equal(bm, want[j][0]), j
+        for tk, j in list(live.items()):
+            srv.wait(tk, 120000)
+            bm, cnt = srv.fetch(tk)
+            assert cnt == want[j][1] and np.array_equal(bm, want[j][0]), j
+        st = srv.stats()
+        assert st["cancelled"] == cancelled > 0
+        assert st["active"] == 0
