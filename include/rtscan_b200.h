@@ -322,7 +322,10 @@ typedef struct rts_server_stats {
   double plan_ms_total; /* host time spent making and uploading them */
 } rts_server_stats;
 
-/* cfg may be NULL (defaults); zero fields take their defaults. */
+/* cfg may be NULL (defaults); zero fields take their defaults.  Beside the
+ * max_active result bitmaps the server holds 32 bytes per segment row for
+ * the shared positions of its passes (268 MB for 2^23-row segments), or
+ * runs without them when that memory is not there. */
 RTS_API rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_server **out);
 /* Queue one conjunctive query; safe from many threads.  RTS_ERR_FULL when the
  * queue holds max_queue requests. */

@@ -72,8 +72,7 @@ struct BatchPlanDeleter {
 using BatchPlanPtr = std::unique_ptr<BatchPlan, BatchPlanDeleter>;
 // share_positions: a plan of several table passes over four columns or
 // fewer searches each row's positions once for all of them (a faster step
-// for a little more host planning; the server, whose steps are bound by
-// re-planning at high rates, plans without).
+// for a little more host planning).
 BatchPlanPtr make_batch_plan(rts_ctx *ctx, const std::vector<NormQuery> &norm, const std::vector<int> &which,
                              const int32_t *out_index, size_t table_budget, bool share_positions);
 // The words to upload to the device before launching.

@@ -76,6 +76,8 @@ struct rts_server {
   int nseg = 0;
   uint32_t *bitmaps = nullptr;
   unsigned long long *counts = nullptr;
+  void *pre = nullptr;  // a segment's shared positions (null: every pass searches)
+  size_t pre_bytes = 0;
   unsigned long long *host_counts = nullptr;  // pinned; slot i's count once it is DONE
   cudaStream_t stream = nullptr, copy_stream = nullptr;
 
@@ -307,9 +309,10 @@ struct rts_server {
     if (!plan || plan_slots.empty()) return;
     const uint64_t r0 = (uint64_t)cursor * seg_rows;
     const uint64_t r1 = std::min<uint64_t>(nrows, r0 + seg_rows);
-    // planned without shared positions (re-planning bounds a busy server's
-    // steps, and they cost more host planning), so no scratch
-    ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, nullptr, 0, stream);
+    // the segment's shared positions, when the plan has them, in the
+    // server's scratch (steps run one after another on the stream)
+    ctx->launches += rts::launch_batch_plan(ctx, *plan, plan_dev, bitmaps, stride, counts, r0, r1, pre, pre_bytes,
+                                            stream);
     RTS_CUDA(cudaGetLastError());
     cudaEvent_t ev = get_event();
     RTS_CUDA(cudaEventRecord(ev, stream));
@@ -406,7 +409,7 @@ struct rts_server {
         }
         if (todo == 1) {  // plan and upload without the lock
           const double t0 = now_s();
-          rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget, false);
+          rts::BatchPlanPtr p = rts::make_batch_plan(ctx, norm, active, nullptr, ctx->batch_cfg.table_budget, true);
           upload(rts::batch_plan_blob(*p));
           const double t1 = now_s();
           std::lock_guard<std::mutex> lk(mu);
@@ -458,6 +461,7 @@ struct rts_server {
     for (auto &kv : ev_refs) cudaEventDestroy(kv.first);  // each slot event once
     if (bitmaps) cudaFree(bitmaps);
     if (counts) cudaFree(counts);
+    if (pre) cudaFree(pre);
     if (host_counts) cudaFreeHost(host_counts);
     if (stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
@@ -532,6 +536,14 @@ rts_status rts_server_start(rts_ctx *ctx, const rts_server_config *cfg, rts_serv
       throw rts::Error(RTS_ERR_NOMEM, "result pool of " + std::to_string(bm_bytes) + " bytes does not fit");
     }
     RTS_CUDA(cudaMallocHost(&srv->host_counts, (size_t)c.max_active * 8));
+    // shared positions of one segment, 8 bytes per row and sharing pass
+    // (268 MB for 2^23-row segments); without it every pass searches
+    srv->pre_bytes = rts::kMaxSharedPasses * (size_t)(c.segment_rows + 2) * 8;
+    if (cudaMalloc(&srv->pre, srv->pre_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      srv->pre = nullptr;
+      srv->pre_bytes = 0;
+    }
     RTS_CUDA(cudaStreamCreateWithFlags(&srv->stream, cudaStreamNonBlocking));
     RTS_CUDA(cudaStreamCreateWithFlags(&srv->copy_stream, cudaStreamNonBlocking));
     srv->slots.resize(c.max_active);

@@ -192,3 +192,19 @@ def test_cancels_while_running_and_slots_reused(ctx, table):
         st = srv.stats()
         assert st["cancelled"] == cancelled > 0
         assert st["active"] == 0
+
+
+def test_many_active_requests_share_positions(ctx, table):
+    """600 requests over the four columns running at once make table passes
+    that share one position search per segment row (the server's segment
+    scratch); every result equals the direct scan."""
+    ctx.load_columns(table)
+    qs = D.batch_queries(table, 600, seed=17, min_cols=2, max_cols=4)
+    want = [alone(ctx, q) for q in qs]
+    with R.Server(ctx, max_active=1024, segment_rows=1 << 18) as srv:
+        tks = [srv.submit(q) for q in qs]
+        for i, tk in enumerate(tks):
+            srv.wait(tk, 120000)
+            bm, cnt = srv.fetch(tk)
+            assert cnt == want[i][1] and np.array_equal(bm, want[i][0]), i
+        assert srv.stats()["plans"] >= 1
