@@ -192,6 +192,47 @@ void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
   CHECK(fed == P.npass, "%d passes fed, %d planned", fed, P.npass);
 }
 
+// batch_plan_drop: a random part of the plan's queries dropped (each a
+// second time too), after which no slot of any pass names a dropped query,
+// every other slot keeps its query, and every reported word is -1 in the
+// blob.
+uint64_t g_dropped = 0;
+void check_drop(rts::BatchPlan &plan, int nq, std::mt19937_64 &rng) {
+  auto slots_of = [&](std::vector<int> &owner) {  // query of every slot, in pass order
+    owner.clear();
+    for (const auto &b : plan.passes) {
+      if (b.few) {
+        for (int j = 0; j < b.fp.nq; j++) owner.push_back(b.fp.slot_query[j]);
+      } else {
+        const int32_t *slot = reinterpret_cast<const int32_t *>(plan.blob.data() + b.off + b.bp.slot_off);
+        for (int sl = 0; sl < 32 * b.groups; sl++) owner.push_back(slot[sl]);
+      }
+    }
+  };
+  std::vector<int> before, after;
+  slots_of(before);
+  std::vector<char> gone(nq, 0);
+  std::vector<uint32_t> words;
+  for (int q = 0; q < nq; q++)
+    if (rng() % 3 == 0) {
+      gone[q] = 1;
+      rts::batch_plan_drop(plan, q, words);
+      rts::batch_plan_drop(plan, q, words);  // a second drop changes nothing
+      g_dropped++;
+    }
+  rts::batch_plan_drop(plan, nq + 5, words);  // a query the plan does not hold
+  slots_of(after);
+  CHECK(before.size() == after.size(), "slot count changed");
+  for (size_t i = 0; i < before.size() && i < after.size(); i++) {
+    const int q = before[i];
+    const int want = q >= 0 && q < nq && gone[q] ? -1 : q;
+    CHECK(after[i] == want, "slot %zu: query %d after drops, want %d", i, after[i], want);
+  }
+  std::sort(words.begin(), words.end());
+  CHECK(std::adjacent_find(words.begin(), words.end()) == words.end(), "a blob word reported twice");
+  for (uint32_t w : words) CHECK(w < plan.blob.size() && plan.blob[w] == 0xFFFFFFFFu, "word %u not cleared", w);
+}
+
 // Bucket indexes of crafted boundary sets: single boundaries at the domain
 // ends, dense runs, wide spreads, and runs crowded into one octave.
 void check_pre_buckets(std::mt19937_64 &rng) {
@@ -297,6 +338,8 @@ int main(int argc, char **argv) {
         else check_table_pass(*plan, b, norm, seen, rng);
       }
       check_pre(*plan, rng);
+      std::mt19937_64 drop_rng(seed * 1000003ull + (uint64_t)t);  // the trials' own stream is left as it was
+      check_drop(*plan, nq, drop_rng);
     }
     for (int q = 0; q < nq; q++) {
       const int want = rts::runs_in_kernel(norm[q]) ? 1 : 0;
@@ -308,9 +351,9 @@ int main(int argc, char **argv) {
     return 1;
   }
   std::printf("planner ok: %d trials, seed %llu: %llu kernel queries, %llu table passes, %llu term-by-term passes, "
-              "%llu mask bits, %llu plans with shared positions (%llu lookups)\n",
+              "%llu mask bits, %llu plans with shared positions (%llu lookups), %llu queries dropped\n",
               trials, (unsigned long long)seed, (unsigned long long)g_kernel_queries, (unsigned long long)g_table_passes,
               (unsigned long long)g_few_passes, (unsigned long long)g_bits, (unsigned long long)g_pre_plans,
-              (unsigned long long)g_pre_lookups);
+              (unsigned long long)g_pre_lookups, (unsigned long long)g_dropped);
   return 0;
 }

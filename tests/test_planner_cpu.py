@@ -53,8 +53,9 @@ def test_planner_invariants(harness, seed):
     assert m, r.stdout
     queries, tables, few, bits = (int(x) for x in m.groups())
     assert queries > 1000 and tables > 0 and few > 0 and bits > 100_000, r.stdout
-    shared = re.search(r"(\d+) plans with shared positions \((\d+) lookups\)", r.stdout)
+    shared = re.search(r"(\d+) plans with shared positions \((\d+) lookups\), (\d+) queries dropped", r.stdout)
     assert shared and int(shared.group(1)) >= 1 and int(shared.group(2)) > 1000, r.stdout
+    assert int(shared.group(3)) > 1000, r.stdout  # batch_plan_drop exercised
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
