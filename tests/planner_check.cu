@@ -10,7 +10,11 @@
 //   * table passes: boundaries sorted and distinct, bmin/bmax their ends,
 //     every mask bit of every used slot equal to the query's verdict on the
 //     interval, every bucket of the index bracketing the true position of
-//     the values it maps, and the pass fitting shared memory.
+//     the values it maps, and the pass fitting shared memory;
+//   * shared positions: every union position and map entry against each
+//     pass's own search;
+//   * dropping queries from a plan (a server's finished requests) leaves no
+//     slot naming them and every other slot as it was.
 // Usage: planner_check SEED TRIALS; exit status 0 when every check holds.
 #include "../rtscan_b200/csrc/batch.cu"
 
