@@ -1024,9 +1024,10 @@ def served_leg(torch, R, D, ctx, dev, rank, args):
         # warm-up
         srv.replay(D.batch_queries(samples, 200, seed=1), np.linspace(0, 0.05, 200))
         for rate in args.serve_rates:
+            rate = int(rate) if float(rate).is_integer() else rate
             nq = max(1, int(rate * seconds))
-            qs = R.prepare(D.batch_queries(samples, nq, seed=rate))
-            arr = np.cumsum(np.random.default_rng(rate).exponential(1.0 / rate, size=nq))
+            qs = R.prepare(D.batch_queries(samples, nq, seed=int(rate)))
+            arr = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, size=nq))
             st0 = srv.stats()
             t0 = time.perf_counter()
             lat = srv.replay(qs, arr)
