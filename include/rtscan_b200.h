@@ -243,7 +243,7 @@ RTS_API rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host
                                        uint64_t *host_counts);
 /* Bytes the context's last rts_scan_batch_host call moved host to device
  * (columns, plan) and device to host (bitmaps: a query whose row chunk has
- * at most one nonzero word in eight travels as (word, value) pairs that the
+ * at most one nonzero word in four travels as (word, value) pairs that the
  * call expands into host_bitmaps; counts).  Zero before the first call. */
 RTS_API rts_status rts_host_transfer_bytes(const rts_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* The same queries with one fused-scan launch per query (the baseline the

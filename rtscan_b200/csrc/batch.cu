@@ -1711,12 +1711,14 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       pre = rts::context_pre_scratch(ctx, pre_bytes, H.compute);
     }
     // Sparse transfer (sparse_d2h.cuh) when a chunk holds enough words per
-    // query; a packed query has at most cw / 8 nonzero words in the chunk.
+    // query; a packed query has at most cw / kSparseDensity nonzero words in
+    // the chunk.
     const uint64_t cw_max = chunk_rows / 32;
     const bool sparse = nq > 0 && !inside.empty() && cw_max >= rts::kSparseMinWords;
     // pairs per chunk: every packed query's, up to kSparseMaxPairs (a query
     // that would pass it is sent whole)
-    const uint64_t max_pairs = sparse ? std::min<uint64_t>((uint64_t)nq * (cw_max / 8), rts::kSparseMaxPairs) : 0;
+    const uint64_t max_pairs =
+        sparse ? std::min<uint64_t>((uint64_t)nq * (cw_max / rts::kSparseDensity), rts::kSparseMaxPairs) : 0;
     if (sparse) {
       rts::ensure(H.nnz, H.nnz_cap, (size_t)nq * nchunks);
       rts::ensure_host(H.nnz_host, H.nnz_host_cap, (size_t)nq * nchunks);
@@ -1755,7 +1757,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
           continue;
         }
         const uint32_t c = try_pack ? H.nnz_host[(size_t)nq * r + q] : 0u;
-        if (try_pack && (uint64_t)c * 8 <= cw && total + c <= max_pairs) {
+        if (try_pack && (uint64_t)c * rts::kSparseDensity <= cw && total + c <= max_pairs) {
           qlh[packed.size()] = q;
           qoh[packed.size()] = total;
           packed.push_back(q);
@@ -1765,7 +1767,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
         }
         int qb = q + 1;  // a run of dense queries
         while (qb < nq && !is_outside[qb] &&
-               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * 8 <= cw &&
+               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * rts::kSparseDensity <= cw &&
                  total + H.nnz_host[(size_t)nq * r + qb] <= max_pairs))
           qb++;
         RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4,

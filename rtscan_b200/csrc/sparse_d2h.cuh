@@ -5,26 +5,29 @@
 // A host-buffer batch call moves every query's bitmap over PCIe, which sets
 // its time (12.5 MB per query at 1e8 rows; the scan itself is about 3 % of
 // the call).  A bitmap of a selective query is mostly zero words: below
-// about 0.4 % of the rows, at most one word in eight is nonzero.  Per row
+// about 0.9 % of the rows, at most one word in four is nonzero.  Per row
 // chunk, after the chunk's scan:
 //   * nnz_kernel counts each query's nonzero words in the chunk, and the
 //     host reads the counts (4 bytes per query) while the next chunk runs;
-//   * a query with at most one nonzero word in eight is sent as the chunk's
-//     (word index, value) pairs in word order, packed by pack_kernel at
-//     offsets the host assigns (8 bytes per nonzero word instead of 4 per
-//     word), and expanded on the host by worker threads (zeros between the
-//     pairs);
+//   * a query with at most one nonzero word in kSparseDensity (four) is
+//     sent as the chunk's (word index, value) pairs in word order, packed by
+//     pack_kernel at offsets the host assigns (8 bytes per nonzero word
+//     instead of 4 per word), and expanded on the host by worker threads
+//     (zeros between the pairs);
 //   * every other query keeps its 2D copy, one per run of consecutive
 //     dense queries.
 // The host's memory takes the worker threads' writes beside the DMA
 // (measured on the B200 box: 55 GB/s of memset beside a 45 GB/s
-// device-to-host copy, against 52 GB/s for the copy alone).
+// device-to-host copy, against 52 GB/s for the copy alone).  On the bench
+// workload (1e8 rows x 4 columns, 1024 queries) a call took 228 / 221 /
+// 208-210 / 208 ms with a word in 16 / 8 / 4 / 3 nonzero as the limit.
 #pragma once
 // (<condition_variable>, <functional>, <mutex> and <thread> come from batch.cu.)
 
 constexpr int kSparseThreads = 256;
 constexpr int kSparseWordsPerThread = 4;
 constexpr uint64_t kSparseMinWords = 4096;  // chunks of fewer words per query are sent whole
+constexpr uint64_t kSparseDensity = 4;      // a packed chunk has at most one nonzero word in this many
 constexpr uint64_t kSparseMaxPairs = 1ull << 24;  // pairs of one chunk (128 MiB per staging slot)
 
 // Nonzero words of query q's bitmap in [w0, w1): one block per query.
