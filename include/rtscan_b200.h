@@ -234,7 +234,8 @@ RTS_API rts_status rts_scan_batch_async(rts_ctx *ctx, const rts_term *terms, con
  * the batched passes, and writes every query's bitmap (host_bitmaps +
  * q*stride_words) and count (host_counts[q]), the download of each row
  * chunk overlapping the next chunk's pass (sparse chunks of a bitmap are
- * sent as pairs and expanded by host threads).  Blocking.  The
+ * sent as a nonzero-word mask and the nonzero words, expanded by host
+ * threads).  Blocking.  The
  * context's resident table is left as it was.  (The reference's per-query
  * upload-scan-download loop, bindex_cuda.cpp:1771-1946.) */
 RTS_API rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host_cols, int32_t ncols,
@@ -242,9 +243,10 @@ RTS_API rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *host
                                        int32_t nqueries, uint32_t *host_bitmaps, uint64_t stride_words,
                                        uint64_t *host_counts);
 /* Bytes the context's last rts_scan_batch_host call moved host to device
- * (columns, plan) and device to host (bitmaps: a query whose row chunk has
- * at most one nonzero word in four travels as (word, value) pairs that the
- * call expands into host_bitmaps; counts).  Zero before the first call. */
+ * (columns, plan) and device to host (bitmaps: a query's row chunk whose
+ * nonzero-word mask, one bit per word, and nonzero words take at most 3/8
+ * of its words travels as those, and the call expands it into
+ * host_bitmaps; counts).  Zero before the first call. */
 RTS_API rts_status rts_host_transfer_bytes(const rts_ctx *ctx, uint64_t *h2d_bytes, uint64_t *d2h_bytes);
 /* The same queries with one fused-scan launch per query (the baseline the
  * batched kernel is measured against). */

@@ -1553,7 +1553,7 @@ struct HostBatchBuffers {
   std::vector<cudaEvent_t> ev;
   // sparse transfer: per chunk the queries' nonzero-word counts (device,
   // pinned host), the packed queries and their pair offsets (pinned host,
-  // device), and the pairs (two device slots, three pinned host slots)
+  // device), and the packed chunks (two device slots, three pinned host slots)
   uint32_t *nnz = nullptr;
   size_t nnz_cap = 0;
   uint32_t *nnz_host = nullptr;
@@ -1566,10 +1566,10 @@ struct HostBatchBuffers {
   size_t ql_host_cap = 0;
   uint64_t *qoff_host = nullptr;
   size_t qoff_host_cap = 0;
-  uint2 *pairs[2] = {nullptr, nullptr};
-  size_t pairs_cap[2] = {0, 0};
-  uint2 *pairs_host[3] = {nullptr, nullptr, nullptr};
-  size_t pairs_host_cap[3] = {0, 0, 0};
+  uint32_t *packed[2] = {nullptr, nullptr};
+  size_t packed_cap[2] = {0, 0};
+  uint32_t *packed_host[3] = {nullptr, nullptr, nullptr};
+  size_t packed_host_cap[3] = {0, 0, 0};
   // bytes the last call moved each way
   uint64_t last_h2d = 0, last_d2h = 0;
   ~HostBatchBuffers() {
@@ -1582,12 +1582,12 @@ struct HostBatchBuffers {
     if (nnz) cudaFree(nnz);
     if (ql) cudaFree(ql);
     if (qoff) cudaFree(qoff);
-    for (auto *pp : pairs)
+    for (auto *pp : packed)
       if (pp) cudaFree(pp);
     if (nnz_host) cudaFreeHost(nnz_host);
     if (ql_host) cudaFreeHost(ql_host);
     if (qoff_host) cudaFreeHost(qoff_host);
-    for (auto *pp : pairs_host)
+    for (auto *pp : packed_host)
       if (pp) cudaFreeHost(pp);
     for (auto e : ev) cudaEventDestroy(e);
     if (up) cudaStreamDestroy(up);
@@ -1682,7 +1682,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     const uint64_t want_chunks = std::max<uint64_t>(1, std::min<uint64_t>(32, nrows >> 22));
     const uint64_t chunk_rows = ((nrows + want_chunks - 1) / want_chunks + 4095) / 4096 * 4096;
     const int nchunks = (int)((nrows + chunk_rows - 1) / chunk_rows);
-    // events per chunk: upload, scan, counts on the host, pack, pairs on the host
+    // events per chunk: upload, scan, counts on the host, pack, packed words on the host
     const int kEv = 5;
     while ((int)H.ev.size() < kEv * nchunks + 1) {
       cudaEvent_t e;
@@ -1697,7 +1697,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     for (int q : outside) is_outside[q] = 1;
     if (nq > 0) RTS_CUDA(cudaMemsetAsync(H.counts, 0, (size_t)nq * 8, H.compute));
     H.last_h2d = (uint64_t)nrows * 4 * ncols;  // and below: the plan, the packed-query lists
-    H.last_d2h = (uint64_t)nq * 8;             // and below: bitmaps, pairs, nonzero-word counts
+    H.last_d2h = (uint64_t)nq * 8;             // and below: bitmaps, packed chunks, nonzero-word counts
     rts::BatchPlan plan;
     const uint32_t *dev_blob = nullptr;
     cudaEvent_t blob_done = nullptr;
@@ -1711,14 +1711,15 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       pre = rts::context_pre_scratch(ctx, pre_bytes, H.compute);
     }
     // Sparse transfer (sparse_d2h.cuh) when a chunk holds enough words per
-    // query; a packed query has at most cw / kSparseDensity nonzero words in
-    // the chunk.
+    // query; a packed query takes at most kPackNum / kPackDen of the chunk's
+    // words.
     const uint64_t cw_max = chunk_rows / 32;
     const bool sparse = nq > 0 && !inside.empty() && cw_max >= rts::kSparseMinWords;
-    // pairs per chunk: every packed query's, up to kSparseMaxPairs (a query
+    // packed words per chunk: every packed query's, up to kSparseMaxWords (a query
     // that would pass it is sent whole)
-    const uint64_t max_pairs =
-        sparse ? std::min<uint64_t>((uint64_t)nq * (cw_max / rts::kSparseDensity), rts::kSparseMaxPairs) : 0;
+    const uint64_t max_packed =
+        sparse ? std::min<uint64_t>((uint64_t)nq * (cw_max * rts::kPackNum / rts::kPackDen), rts::kSparseMaxWords)
+               : 0;
     if (sparse) {
       rts::ensure(H.nnz, H.nnz_cap, (size_t)nq * nchunks);
       rts::ensure_host(H.nnz_host, H.nnz_host_cap, (size_t)nq * nchunks);
@@ -1726,8 +1727,8 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       rts::ensure(H.qoff, H.qoff_cap, (size_t)nq * nchunks);
       rts::ensure_host(H.ql_host, H.ql_host_cap, (size_t)nq * nchunks);
       rts::ensure_host(H.qoff_host, H.qoff_host_cap, (size_t)nq * nchunks);
-      for (int i = 0; i < 2; i++) rts::ensure(H.pairs[i], H.pairs_cap[i], (size_t)max_pairs);
-      for (int i = 0; i < 3; i++) rts::ensure_host(H.pairs_host[i], H.pairs_host_cap[i], (size_t)max_pairs);
+      for (int i = 0; i < 2; i++) rts::ensure(H.packed[i], H.packed_cap[i], (size_t)max_packed);
+      for (int i = 0; i < 3; i++) rts::ensure_host(H.packed_host[i], H.packed_host_cap[i], (size_t)max_packed);
     }
     // Host threads that expand packed queries (declared after the buffers'
     // owner, so that they are joined on every way out before the streams
@@ -1740,7 +1741,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
     }
     // Finish chunk r once its counts are on the host: the dense queries'
     // words leave as one 2D copy per run of consecutive dense queries, the
-    // packed ones as pairs expanded by the pool.
+    // packed ones as masks and values expanded by the pool.
     auto finish = [&](int r) {
       const uint64_t r0 = (uint64_t)r * chunk_rows, r1 = std::min<uint64_t>(nrows, r0 + chunk_rows);
       const uint64_t w0 = r0 / 32, w1 = r1 == nrows ? words : r1 / 32, cw = w1 - w0;
@@ -1750,14 +1751,22 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       if (try_pack) RTS_CUDA(cudaEventSynchronize(ev(r, 2)));
       int32_t *qlh = H.ql_host + (size_t)nq * r;
       uint64_t *qoh = H.qoff_host + (size_t)nq * r;
+      // a packed query's words: its mask (one bit per word) and its nonzero
+      // words; it is packed when they take at most kPackNum / kPackDen of the
+      // chunk and fit the staging slot
+      auto packed_words = [&](int i) { return (cw + 31) / 32 + H.nnz_host[(size_t)nq * r + i]; };
+      auto packs = [&](int i) {
+        return try_pack && packed_words(i) * rts::kPackDen <= cw * rts::kPackNum &&
+               total + packed_words(i) <= max_packed;
+      };
       int q = 0;
       while (q < nq) {
         if (is_outside[q]) {
           q++;
           continue;
         }
-        const uint32_t c = try_pack ? H.nnz_host[(size_t)nq * r + q] : 0u;
-        if (try_pack && (uint64_t)c * rts::kSparseDensity <= cw && total + c <= max_pairs) {
+        if (packs(q)) {
+          const uint64_t c = packed_words(q);
           qlh[packed.size()] = q;
           qoh[packed.size()] = total;
           packed.push_back(q);
@@ -1766,10 +1775,7 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
           continue;
         }
         int qb = q + 1;  // a run of dense queries
-        while (qb < nq && !is_outside[qb] &&
-               !(try_pack && (uint64_t)H.nnz_host[(size_t)nq * r + qb] * rts::kSparseDensity <= cw &&
-                 total + H.nnz_host[(size_t)nq * r + qb] <= max_pairs))
-          qb++;
+        while (qb < nq && !is_outside[qb] && !packs(qb)) qb++;
         RTS_CUDA(cudaMemcpy2DAsync(host_bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4,
                                    H.bitmaps + (uint64_t)q * stride_words + w0, stride_words * 4, cw * 4,
                                    (size_t)(qb - q), cudaMemcpyDeviceToHost, H.copy));
@@ -1786,29 +1792,27 @@ extern "C" rts_status rts_scan_batch_host(rts_ctx *ctx, const uint32_t *const *h
       RTS_CUDA(cudaMemcpyAsync(qod, qoh, np * sizeof(uint64_t), cudaMemcpyHostToDevice, H.compute));
       H.last_h2d += (uint64_t)np * (sizeof(int32_t) + sizeof(uint64_t));
       if (r >= 2) RTS_CUDA(cudaStreamWaitEvent(H.compute, ev(r - 2, 4), 0));  // the device slot's last copy
-      rts::pack_kernel<<<np, rts::kSparseThreads, 0, H.compute>>>(H.bitmaps, stride_words, w0, w1, qld, qod,
-                                                                H.pairs[ds]);
+      rts::pack_kernel<<<np, rts::kPackThreads, 0, H.compute>>>(H.bitmaps, stride_words, w0, w1, qld, qod,
+                                                               H.packed[ds]);
       ctx->launches++;
       RTS_CUDA(cudaEventRecord(ev(r, 3), H.compute));
       RTS_CUDA(cudaStreamWaitEvent(H.copy, ev(r, 3), 0));
       if (total)
-        RTS_CUDA(cudaMemcpyAsync(H.pairs_host[hs], H.pairs[ds], total * sizeof(uint2), cudaMemcpyDeviceToHost,
+        RTS_CUDA(cudaMemcpyAsync(H.packed_host[hs], H.packed[ds], total * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  H.copy));
-      H.last_d2h += total * sizeof(uint2);
+      H.last_d2h += total * sizeof(uint32_t);
       RTS_CUDA(cudaEventRecord(ev(r, 4), H.copy));
       const int tasks = std::min(np, pool->size());
       gate.add(hs, tasks);
       cudaEvent_t e = ev(r, 4);
-      const uint2 *ph = H.pairs_host[hs];
+      const uint32_t *ph = H.packed_host[hs];
       const int dev = ctx->device;
       for (int t = 0; t < tasks; t++)
         pool->post([=, &gate] {
           cudaSetDevice(dev);
           cudaEventSynchronize(e);
-          for (int j = t; j < np; j += tasks) {
-            const uint64_t a = qoh[j], b = j + 1 < np ? qoh[j + 1] : total;
-            rts::expand_pairs(host_bitmaps + (uint64_t)qlh[j] * stride_words + w0, cw, ph + a, b - a);
-          }
+          for (int j = t; j < np; j += tasks)
+            rts::expand_mask(host_bitmaps + (uint64_t)qlh[j] * stride_words + w0, cw, ph + qoh[j]);
           gate.done(hs);
         });
     };

@@ -1,34 +1,32 @@
-// Sparse result bitmaps leave the device as (word, value) pairs (included
-// by batch.cu inside its anonymous namespace in rts; used by
-// rts_scan_batch_host).
+// Sparse result bitmaps leave the device packed as a nonzero-word mask and
+// the nonzero words (included by batch.cu inside its anonymous namespace in
+// rts; used by rts_scan_batch_host).
 //
 // A host-buffer batch call moves every query's bitmap over PCIe, which sets
 // its time (12.5 MB per query at 1e8 rows; the scan itself is about 3 % of
-// the call).  A bitmap of a selective query is mostly zero words: below
-// about 0.9 % of the rows, at most one word in four is nonzero.  Per row
+// the call).  A bitmap of a selective query is mostly zero words.  Per row
 // chunk, after the chunk's scan:
 //   * nnz_kernel counts each query's nonzero words in the chunk, and the
 //     host reads the counts (4 bytes per query) while the next chunk runs;
-//   * a query with at most one nonzero word in kSparseDensity (four) is
-//     sent as the chunk's (word index, value) pairs in word order, packed by
-//     pack_kernel at offsets the host assigns (8 bytes per nonzero word
-//     instead of 4 per word), and expanded on the host by worker threads
-//     (zeros between the pairs);
+//   * a query whose mask (one bit per word) and nonzero words take at most
+//     kPackNum / kPackDen (3/8) of the chunk's words is packed by
+//     pack_kernel at the offset the host assigns, and expanded on the host
+//     by worker threads (zeros where the mask bit is clear);
 //   * every other query keeps its 2D copy, one per run of consecutive
 //     dense queries.
 // The host's memory takes the worker threads' writes beside the DMA
 // (measured on the B200 box: 55 GB/s of memset beside a 45 GB/s
-// device-to-host copy, against 52 GB/s for the copy alone).  On the bench
-// workload (1e8 rows x 4 columns, 1024 queries) a call took 228 / 221 /
-// 208-210 / 208 ms with a word in 16 / 8 / 4 / 3 nonzero as the limit.
+// device-to-host copy, against 52 GB/s for the copy alone).
 #pragma once
 // (<condition_variable>, <functional>, <mutex> and <thread> come from batch.cu.)
 
 constexpr int kSparseThreads = 256;
 constexpr int kSparseWordsPerThread = 4;
 constexpr uint64_t kSparseMinWords = 4096;  // chunks of fewer words per query are sent whole
-constexpr uint64_t kSparseDensity = 4;      // a packed chunk has at most one nonzero word in this many
-constexpr uint64_t kSparseMaxPairs = 1ull << 24;  // pairs of one chunk (128 MiB per staging slot)
+// a chunk is packed when its mask and values take at most kPackNum /
+// kPackDen of its words
+constexpr uint64_t kPackNum = 3, kPackDen = 8;
+constexpr uint64_t kSparseMaxWords = 1ull << 25;  // packed words of one chunk (128 MiB per staging slot)
 
 // Nonzero words of query q's bitmap in [w0, w1): one block per query.
 __global__ void __launch_bounds__(kSparseThreads) nnz_kernel(const uint32_t *bm, uint64_t stride, uint64_t w0,
@@ -56,47 +54,42 @@ __global__ void __launch_bounds__(kSparseThreads) nnz_kernel(const uint32_t *bm,
   }
 }
 
-// The nonzero words of query ql[j] in [w0, w1) as (word - w0, value) pairs
-// in word order at out + off[j]: one block per listed query, tiles of
-// kSparseThreads * kSparseWordsPerThread words, each thread four
-// consecutive words, ranks by a block-wide prefix of the threads' counts.
-__global__ void __launch_bounds__(kSparseThreads) pack_kernel(const uint32_t *bm, uint64_t stride, uint64_t w0,
-                                                              uint64_t w1, const int32_t *ql, const uint64_t *off,
-                                                              uint2 *out) {
-  const uint32_t *p = bm + (uint64_t)ql[blockIdx.x] * stride;
-  uint2 *o = out + off[blockIdx.x];
-  __shared__ uint32_t wsum[kSparseThreads / 32];
+// Query ql[j]'s words [w0, w1) as a nonzero mask (bit k of mask word i:
+// word 32i + k is nonzero) followed by the nonzero words in order, at
+// out + off[j]: one block per listed query, one word per thread per tile of
+// kPackThreads words, a warp's ballot its mask word, ranks by a block-wide
+// prefix of the warps' counts.
+constexpr int kPackThreads = 1024;
+__global__ void __launch_bounds__(kPackThreads) pack_kernel(const uint32_t *bm, uint64_t stride, uint64_t w0,
+                                                            uint64_t w1, const int32_t *ql, const uint64_t *off,
+                                                            uint32_t *out) {
+  const uint32_t *p = bm + (uint64_t)ql[blockIdx.x] * stride + w0;
+  const uint64_t cw = w1 - w0, nm = (cw + 31) / 32;
+  uint32_t *mask = out + off[blockIdx.x];
+  uint32_t *vals = mask + nm;
+  __shared__ uint32_t wcnt[kPackThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint64_t base = 0;
-  constexpr uint64_t kTile = (uint64_t)kSparseThreads * kSparseWordsPerThread;
-  for (uint64_t t0 = w0; t0 < w1; t0 += kTile) {
-    const uint64_t w = t0 + (uint64_t)threadIdx.x * kSparseWordsPerThread;
-    uint32_t v[kSparseWordsPerThread];
-    uint32_t c = 0;
-#pragma unroll
-    for (int k = 0; k < kSparseWordsPerThread; k++) {
-      v[k] = w + k < w1 ? __ldg(p + w + k) : 0u;
-      c += v[k] != 0;
+  for (uint64_t t0 = 0; t0 < cw; t0 += kPackThreads) {
+    const uint64_t i = t0 + threadIdx.x;
+    const uint32_t v = i < cw ? __ldg(p + i) : 0u;
+    const uint32_t b = __ballot_sync(0xFFFFFFFFu, v != 0);
+    if (lane == 0) {
+      if (t0 / 32 + warp < nm) mask[t0 / 32 + warp] = b;
+      wcnt[warp] = __popc(b);
     }
-    uint32_t incl = c;  // inclusive prefix over the warp
+    __syncthreads();
+    uint32_t incl = wcnt[lane];  // every warp scans the warps' counts
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
       if (lane >= d) incl += y;
     }
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    uint32_t before = 0, total = 0;
-    for (int i = 0; i < kSparseThreads / 32; i++) {
-      before += i < warp ? wsum[i] : 0u;
-      total += wsum[i];
-    }
-    uint64_t r = base + before + incl - c;
-#pragma unroll
-    for (int k = 0; k < kSparseWordsPerThread; k++)
-      if (v[k]) o[r++] = make_uint2((uint32_t)(w + k - w0), v[k]);
+    const uint32_t before = __shfl_sync(0xFFFFFFFFu, incl, warp) - wcnt[warp];
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (v) vals[base + before + __popc(b & ((1u << lane) - 1u))] = v;
     base += total;
-    __syncthreads();  // wsum is rewritten by the next tile
+    __syncthreads();  // wcnt is rewritten by the next tile
   }
 }
 
@@ -170,15 +163,15 @@ class SlotGate {
   int busy_[8] = {0};
 };
 
-// Query q's chunk [w0, w0 + cw) of the host bitmap from its pairs: zeros
-// between them.
-inline void expand_pairs(uint32_t *dst, uint64_t cw, const uint2 *pairs, uint64_t n) {
-  uint64_t cur = 0;
-  for (uint64_t i = 0; i < n; i++) {
-    const uint64_t w = pairs[i].x;
-    if (w > cur) memset(dst + cur, 0, (w - cur) * 4);
-    dst[w] = pairs[i].y;
-    cur = w + 1;
+// Query q's chunk of cw words of the host bitmap from its mask and values
+// (pack_kernel's layout): the chunk is zeroed, then each set mask bit's word
+// is stored.
+inline void expand_mask(uint32_t *dst, uint64_t cw, const uint32_t *packed) {
+  const uint64_t nm = (cw + 31) / 32;
+  const uint32_t *vals = packed + nm;
+  memset(dst, 0, cw * 4);
+  for (uint64_t i = 0; i < nm; i++) {
+    uint32_t *d = dst + 32 * i;
+    for (uint32_t m = packed[i]; m; m &= m - 1) d[__builtin_ctz(m)] = *vals++;
   }
-  if (cur < cw) memset(dst + cur, 0, (cw - cur) * 4);
 }

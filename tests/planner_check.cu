@@ -14,7 +14,9 @@
 //   * shared positions: every union position and map entry against each
 //     pass's own search;
 //   * dropping queries from a plan (a server's finished requests) leaves no
-//     slot naming them and every other slot as it was.
+//     slot naming them and every other slot as it was;
+//   * a host-buffer batch's packed row chunk (nonzero-word mask, then the
+//     nonzero words) expands to the chunk's words and writes nothing past it.
 // Usage: planner_check SEED TRIALS; exit status 0 when every check holds.
 #include "../rtscan_b200/csrc/batch.cu"
 
@@ -262,6 +264,35 @@ void check_pre_buckets(std::mt19937_64 &rng) {
   }
 }
 
+uint64_t g_expanded = 0;
+// Chunks of random length and density, packed as pack_kernel lays them out
+// (bit k of mask word i set when word 32i + k is nonzero; the nonzero words
+// follow in order), expanded by the host's expand_mask into a buffer of ones.
+void check_expand_mask(std::mt19937_64 &rng) {
+  const uint64_t lens[] = {1, 31, 32, 33, 1000, 4096, 4097, 65536 + 17};
+  for (uint64_t cw : lens)
+    for (int density : {0, 1, 8, 64, 200, 256}) {  // nonzero words per 256
+      std::vector<uint32_t> words(cw);
+      for (auto &w : words) w = (int)(rng() % 256) < density ? (uint32_t)(rng() | 1) : 0u;
+      if (density == 256 && cw > 40) words[cw / 2] = 0;  // one zero among full mask words
+      const uint64_t nm = (cw + 31) / 32;
+      std::vector<uint32_t> packed(nm, 0u);
+      for (uint64_t i = 0; i < cw; i++)
+        if (words[i]) {
+          packed[i / 32] |= 1u << (i % 32);
+          packed.push_back(words[i]);
+        }
+      std::vector<uint32_t> out(cw + 8, 0xFFFFFFFFu);
+      rts::expand_mask(out.data(), cw, packed.data());
+      CHECK(std::equal(words.begin(), words.end(), out.begin()), "expand_mask: %llu words, density %d differ",
+            (unsigned long long)cw, density);
+      for (uint64_t i = cw; i < cw + 8; i++)
+        CHECK(out[i] == 0xFFFFFFFFu, "expand_mask: %llu words, density %d: word %llu past the chunk written",
+              (unsigned long long)cw, density, (unsigned long long)i);
+      g_expanded += cw;
+    }
+}
+
 void check_few_pass(const rts::BatchPlan::Pass &b, const std::vector<rts::NormQuery> &norm, std::vector<int> &seen) {
   const rts::FewPass &f = b.fp;
   g_few_passes++;
@@ -292,6 +323,8 @@ int main(int argc, char **argv) {
   const int trials = argc > 2 ? std::atoi(argv[2]) : 20;
   std::mt19937_64 rng(seed);
   check_pre_buckets(rng);
+  std::mt19937_64 pack_rng(seed ^ 0x5eed5eedull);  // the trials' own stream is left as it was
+  check_expand_mask(pack_rng);
   const int counts[] = {1, 2, 3, 4, 20, 21, 32, 100, 128, 129, 200, 256, 257, 400, 512, 513, 700, 1100};
   for (int t = 0; t < trials; t++) {
     auto *ctx = new rts_ctx();  // never destroyed: it owns no device memory
@@ -355,9 +388,11 @@ int main(int argc, char **argv) {
     return 1;
   }
   std::printf("planner ok: %d trials, seed %llu: %llu kernel queries, %llu table passes, %llu term-by-term passes, "
-              "%llu mask bits, %llu plans with shared positions (%llu lookups), %llu queries dropped\n",
+              "%llu mask bits, %llu plans with shared positions (%llu lookups), %llu queries dropped, "
+              "%llu packed words expanded\n",
               trials, (unsigned long long)seed, (unsigned long long)g_kernel_queries, (unsigned long long)g_table_passes,
               (unsigned long long)g_few_passes, (unsigned long long)g_bits, (unsigned long long)g_pre_plans,
-              (unsigned long long)g_pre_lookups, (unsigned long long)g_dropped);
+              (unsigned long long)g_pre_lookups, (unsigned long long)g_dropped,
+              (unsigned long long)g_expanded);
   return 0;
 }

@@ -64,7 +64,7 @@ def test_cpu_baseline_and_e2e(line):
     words = (n + 31) // 32
     assert e["unit"] == line["unit"]
     # what the call moved: every column up (plus the plan), the bitmaps down,
-    # sparse row chunks as (word, value) pairs, so at most the whole bitmaps
+    # sparse row chunks as nonzero-word masks and values, so at most the whole bitmaps
     # and counts plus the per-chunk nonzero-word counts
     assert 4 * n * ncols <= e["h2d_bytes_per_step"] < 4 * n * ncols * 1.01
     assert e["dense_d2h_bytes_per_step"] == nq * (words * 4 + 8)

@@ -336,8 +336,8 @@ def test_four_passes_share_positions(ctx):
 
 
 def test_batch_host_sparse_chunks_are_expanded(ctx):
-    """Row chunks whose bitmap words are mostly zero leave the device as
-    (word, value) pairs that host threads expand: into buffers filled with
+    """Row chunks whose bitmap words are mostly zero leave the device as a
+    nonzero-word mask and the nonzero words, which host threads expand: into buffers filled with
     ones beforehand, every bitmap (very selective, dense and outside-kernel
     queries mixed, four chunks) equals the device path's, the padding after
     each bitmap is untouched, and fewer bytes crossed than whole bitmaps."""
