@@ -282,14 +282,19 @@ void check_expand_mask(std::mt19937_64 &rng) {
           packed[i / 32] |= 1u << (i % 32);
           packed.push_back(words[i]);
         }
-      std::vector<uint32_t> out(cw + 8, 0xFFFFFFFFu);
-      rts::expand_mask(out.data(), cw, packed.data());
-      CHECK(std::equal(words.begin(), words.end(), out.begin()), "expand_mask: %llu words, density %d differ",
-            (unsigned long long)cw, density);
-      for (uint64_t i = cw; i < cw + 8; i++)
-        CHECK(out[i] == 0xFFFFFFFFu, "expand_mask: %llu words, density %d: word %llu past the chunk written",
-              (unsigned long long)cw, density, (unsigned long long)i);
-      g_expanded += cw;
+      for (int off = 0; off < 4; off++) {  // destinations at every 4-byte offset from a 16-byte boundary
+        std::vector<uint32_t> out(cw + 16, 0xFFFFFFFFu);
+        uint32_t *base = out.data();
+        while ((uintptr_t)base & 15) base++;
+        rts::expand_mask(base + off, cw, packed.data());
+        CHECK(std::equal(words.begin(), words.end(), base + off), "expand_mask: %llu words, density %d, offset %d differ",
+              (unsigned long long)cw, density, off);
+        for (uint32_t *w = out.data(); w < out.data() + out.size(); w++)
+          CHECK(*w == 0xFFFFFFFFu || (w >= base + off && w < base + off + cw),
+                "expand_mask: %llu words, density %d, offset %d: a word outside the chunk written",
+                (unsigned long long)cw, density, off);
+        g_expanded += cw;
+      }
     }
 }
 
