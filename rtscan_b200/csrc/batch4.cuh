@@ -22,10 +22,11 @@
 //      words for the block (128 bytes per 1024 rows) leave as 16-byte stores
 //      from 128 / GV lanes, whole 128-byte lines.
 // No cross-lane exchange is needed, and positions are shared by all queries
-// of the pass.  The 512-slot, 16-warp pass over four columns that reads
-// shared positions runs step 2 with wide lanes (16 rows x two groups, 8-byte
-// table loads, 16-bit stage halves; see the kernel): its loads per mask bit
-// are halved, which measured 2.9 % faster per 1024-query step.  For 512- and 256-slot passes over up to 4 columns, step 1
+// of the pass.  512-slot, 16-warp passes over up to four columns run step 2
+// with wide lanes (16 rows x two groups, 8-byte table loads, 16-bit stage
+// halves; see the kernel): their loads per mask bit are halved, which
+// measured 2.9 % faster per 1024-query step (passes reading shared
+// positions) and 1.8 % faster for 400- and 512-query batches.  For 512- and 256-slot passes over up to 4 columns, step 1
 // for the next block runs inside step 2 (see the kernel).
 template <int GV, int W>
 struct V4Shape {
@@ -198,11 +199,11 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
 #pragma unroll
     for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[c] * GV : 0u;
   };
-  // Wide pass (512 slots, 16 warps, four columns, shared positions): a lane
-  // takes 16 rows and 64 slots (two groups) of step 2, with 8-byte table
-  // loads; see step 2.  The position buffer then has a padding row per 16
+  // Wide pass (512 slots, 16 warps, up to four columns): a lane takes 16
+  // rows and 64 slots (two groups) of step 2, with 8-byte table loads; see
+  // step 2.  The position buffer then has a padding row per 16
   // rows, so that the four 16-row tiles of a warp read it in different banks.
-  constexpr bool kWide = PRE && GV == 16 && W == 16 && CMAX == 4;
+  constexpr bool kWide = GV == 16 && W == 16 && CMAX == 4;
   auto pos_row = [](int r) { return kWide ? r + (r >> 4) : r + (r >> 5); };
   auto put_row = [&](int h, const uint32_t(&off)[CMAX]) {
     const int r = threadIdx.x + h * kV4Threads;
