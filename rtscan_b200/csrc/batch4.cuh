@@ -22,8 +22,8 @@
 //      words for the block (128 bytes per 1024 rows) leave as 16-byte stores
 //      from 128 / GV lanes, whole 128-byte lines.
 // No cross-lane exchange is needed, and positions are shared by all queries
-// of the pass.  512-slot, 16-warp passes over up to four columns run step 2
-// with wide lanes (16 rows x two groups, 8-byte table loads, 16-bit stage
+// of the pass.  256- and 512-slot, 16-warp passes over up to four columns
+// run step 2 with wide lanes (16 rows x two groups, 8-byte table loads, 16-bit stage
 // halves; see the kernel): their loads per mask bit are halved, which
 // measured 2.9 % faster per 1024-query step (passes reading shared
 // positions) and 1.8 % faster for 400- and 512-query batches.  For 512- and 256-slot passes over up to 4 columns, step 1
@@ -56,11 +56,11 @@ struct V4Shape {
 // under 2^16 words), one padding row per tile.
 template <int CMAX>
 using V4Pos = typename std::conditional<(CMAX <= 4), uint32_t, uint16_t>::type;
-// (512 slots on 16 warps over four columns: one padding row per 16, for
-// the wide pass that reads shared positions; see batch4_kernel)
+// (256 or 512 slots on 16 warps over up to four columns: one padding row
+// per 16, for the wide lanes of batch4_kernel)
 template <int CMAX, int GV, int W>
 constexpr int kV4PosBytes =
-    (V4Shape<GV, W>::kRows + ((GV == 16 && W == 16 && CMAX == 4) ? V4Shape<GV, W>::kRows / 16 : V4Shape<GV, W>::kTiles)) *
+    (V4Shape<GV, W>::kRows + ((GV >= 8 && W == 16 && CMAX == 4) ? V4Shape<GV, W>::kRows / 16 : V4Shape<GV, W>::kTiles)) *
     CMAX * (int)sizeof(V4Pos<CMAX>);
 
 // Exchange the bits of a under mask M << S with the bits of b under M (a
@@ -199,11 +199,11 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
 #pragma unroll
     for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[c] * GV : 0u;
   };
-  // Wide pass (512 slots, 16 warps, up to four columns): a lane takes 16
+  // Wide pass (256 or 512 slots, 16 warps, up to four columns): a lane takes 16
   // rows and 64 slots (two groups) of step 2, with 8-byte table loads; see
   // step 2.  The position buffer then has a padding row per 16
   // rows, so that the four 16-row tiles of a warp read it in different banks.
-  constexpr bool kWide = GV == 16 && W == 16 && CMAX == 4;
+  constexpr bool kWide = (GV == 16 || GV == 8) && W == 16 && CMAX == 4;
   auto pos_row = [](int r) { return kWide ? r + (r >> 4) : r + (r >> 5); };
   auto put_row = [&](int h, const uint32_t(&off)[CMAX]) {
     const int r = threadIdx.x + h * kV4Threads;
@@ -343,15 +343,16 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
     };
     if (!(warp & 1)) ahead();
     if constexpr (kWide) {
-      // Wide lanes: 16-row tile k = lane >> 3 of the warp (rows 16hh .. 16hh + 15
-      // of the block's 32-row tile T = 2 * warp + (k & 1), hh = k >> 1) and
-      // groups 2gp, 2gp + 1 (gp = lane & 7): one 8-byte table load per row
+      // Wide lanes: 16-row tile k = lane / (GV / 2) of the warp (rows
+      // 16hh .. 16hh + 15 of the block's 32-row tile T = kTPW * warp +
+      // k % kTPW, hh = k / kTPW) and groups 2gp, 2gp + 1 (gp = lane %
+      // (GV / 2)): one 8-byte table load per row
       // and column serves both groups, half the loads per mask bit of the
       // 32-row, one-group lanes; the two 16 x 32 masks are transposed as
       // 16 x 16 blocks in 16-bit halves and written to the stage as 16-bit
       // halves of its words (rows 0-15 the high half).
-      const int k = lane >> 3, gp = lane & 7;
-      const int T = 2 * warp + (k & 1), hh = k >> 1;
+      const int k = lane / (GV / 2), gp = lane % (GV / 2);
+      const int T = S::kTPW * warp + (k % S::kTPW), hh = k / S::kTPW;
       const int row0 = 32 * T + 16 * hh;
       const char *tabg = reinterpret_cast<const char *>(blob + 2 * gp);
       uint32_t x0[16], x1[16];
