@@ -162,7 +162,7 @@ void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
     return;
   }
   g_pre_plans++;
-  CHECK(P.npass >= 2 && P.npass <= rts::kMaxPrePasses, "%d passes share positions", P.npass);
+  CHECK(P.npass >= 1 && P.npass <= rts::kMaxPrePasses, "%d passes share positions", P.npass);
   CHECK(P.ncols >= 1 && P.ncols <= 4, "%d union columns", P.ncols);
   const uint32_t *ub = plan.blob.data() + plan.pre_off;
   const int NW = (P.npass + 1) / 2;
