@@ -567,10 +567,12 @@ void launch_shape4(const BatchPass &bp, int groups, int sm_count, cudaStream_t s
 void launch_pre4(const BatchPass &bp, int groups, int warps, int sm_count, cudaStream_t s) {
   if (warps == 8) {
     if (groups == 16) launch_one4<4, 16, 8, true>(bp, sm_count, s);
-    else launch_one4<4, 8, 8, true>(bp, sm_count, s);
+    else if (groups == 8) launch_one4<4, 8, 8, true>(bp, sm_count, s);
+    else launch_one4<4, 4, 8, true>(bp, sm_count, s);
   } else {
     if (groups == 16) launch_one4<4, 16, 16, true>(bp, sm_count, s);
-    else launch_one4<4, 8, 16, true>(bp, sm_count, s);
+    else if (groups == 8) launch_one4<4, 8, 16, true>(bp, sm_count, s);
+    else launch_one4<4, 4, 16, true>(bp, sm_count, s);
   }
 }
 
@@ -988,7 +990,7 @@ void plan_shared_positions(BatchPlan &plan) {
   std::vector<int> which;
   for (size_t i = 0; i < plan.passes.size() && (int)which.size() < kMaxPrePasses; i++) {
     const BatchPlan::Pass &b = plan.passes[i];
-    if (b.few || b.variant != 4 || b.cmax != 4 || b.groups < 8) continue;
+    if (b.few || b.variant != 4 || b.cmax != 4) continue;
     if (!which.empty()) {
       const BatchPass &f = plan.passes[which[0]].bp;
       if (b.bp.ncols != f.ncols) continue;

@@ -22,12 +22,14 @@
 //      words for the block (128 bytes per 1024 rows) leave as 16-byte stores
 //      from 128 / GV lanes, whole 128-byte lines.
 // No cross-lane exchange is needed, and positions are shared by all queries
-// of the pass.  256- and 512-slot, 16-warp passes over up to four columns
-// run step 2 with wide lanes (16 rows x two groups, 8-byte table loads, 16-bit stage
+// of the pass.  16-warp passes over up to four columns run step 2 with
+// wide lanes (16 rows x two groups, 8-byte table loads, 16-bit stage
 // halves; see the kernel): their loads per mask bit are halved, which
 // measured 2.9 % faster per 1024-query step (passes reading shared
-// positions) and 1.8 % faster for 400- and 512-query batches.  For 512- and 256-slot passes over up to 4 columns, step 1
-// for the next block runs inside step 2 (see the kernel).
+// positions), 1.8 % faster for 400- and 512-query batches and 20-22 %
+// faster for 64- and 128-query ones.  For 512- and 256-slot passes over up
+// to 4 columns, and every pass reading shared positions, step 1 for the
+// next block runs inside step 2 (see the kernel).
 template <int GV, int W>
 struct V4Shape {
   static_assert(GV == 16 || GV == 8 || GV == 4, "512-, 256- or 128-slot passes");
@@ -56,11 +58,11 @@ struct V4Shape {
 // under 2^16 words), one padding row per tile.
 template <int CMAX>
 using V4Pos = typename std::conditional<(CMAX <= 4), uint32_t, uint16_t>::type;
-// (256 or 512 slots on 16 warps over up to four columns: one padding row
-// per 16, for the wide lanes of batch4_kernel)
+// (16 warps over up to four columns: one padding row per 16, for the wide
+// lanes of batch4_kernel)
 template <int CMAX, int GV, int W>
 constexpr int kV4PosBytes =
-    (V4Shape<GV, W>::kRows + ((GV >= 8 && W == 16 && CMAX == 4) ? V4Shape<GV, W>::kRows / 16 : V4Shape<GV, W>::kTiles)) *
+    (V4Shape<GV, W>::kRows + ((W == 16 && CMAX == 4) ? V4Shape<GV, W>::kRows / 16 : V4Shape<GV, W>::kTiles)) *
     CMAX * (int)sizeof(V4Pos<CMAX>);
 
 // Exchange the bits of a under mask M << S with the bits of b under M (a
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
   // 16-bit pairs until the next step 1 writes them to shared memory, and the
   // column values are loaded one more block ahead.  Other shapes find the
   // positions of a block in its own step 1.
-  constexpr bool kAhead = (GV == 16 || GV == 8) && CMAX <= 4;
+  constexpr bool kAhead = (GV == 16 || GV == 8 || PRE) && CMAX <= 4;
   static_assert(!PRE || (kAhead && CMAX == 4), "shared positions feed the 4-column look-ahead shapes");
   uint32_t val[S::kRPT][CMAX];                    // column values of this thread's rows (PRE: packed offsets)
   uint32_t offn[kAhead ? S::kRPT : 1][(CMAX + 1) / 2];  // their table word offsets, two per register
@@ -199,11 +201,11 @@ __global__ void __launch_bounds__(W * 32, 16 / W) batch4_kernel(const __grid_con
 #pragma unroll
     for (int c = 0; c < CMAX; c++) off[c] = c < C ? p.tab_off[c] + pos[c] * GV : 0u;
   };
-  // Wide pass (256 or 512 slots, 16 warps, up to four columns): a lane takes 16
+  // Wide pass (16 warps, up to four columns): a lane takes 16
   // rows and 64 slots (two groups) of step 2, with 8-byte table loads; see
   // step 2.  The position buffer then has a padding row per 16
   // rows, so that the four 16-row tiles of a warp read it in different banks.
-  constexpr bool kWide = (GV == 16 || GV == 8) && W == 16 && CMAX == 4;
+  constexpr bool kWide = W == 16 && CMAX == 4;
   auto pos_row = [](int r) { return kWide ? r + (r >> 4) : r + (r >> 5); };
   auto put_row = [&](int h, const uint32_t(&off)[CMAX]) {
     const int r = threadIdx.x + h * kV4Threads;

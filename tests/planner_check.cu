@@ -175,7 +175,7 @@ void check_pre(const rts::BatchPlan &plan, std::mt19937_64 &rng) {
     fed++;
     const int q = b.pre_slot;
     CHECK(q < P.npass, "pass slot %d of %d", q, P.npass);
-    CHECK(!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 8, "shared positions feed a pass of shape %d/%d",
+    CHECK(!b.few && b.variant == 4 && b.cmax == 4 && b.groups >= 4, "shared positions feed a pass of shape %d/%d",
           b.cmax, b.groups);
     CHECK(b.bp.ncols == P.ncols, "a pass of %d columns fed by %d union columns", b.bp.ncols, P.ncols);
     const uint32_t *pblob = plan.blob.data() + b.off;
